@@ -1,0 +1,195 @@
+"""Seeded synthetic initial states for the benchmark configurations.
+
+The reference builds its initial states with per-model code
+(``models/init_user.cu.*``, ``models/initialisation_user.h.*``) or reads VAC
+config files; these generators produce the same kind of state directly, in the
+reference's storage layout:
+
+    w[f, k, j, i]   field-major, x fastest, 2 ghost layers per side,
+    2-D fields  rho m1 m2 e b1 b2 eb rhob b1b b2b          (iotypes.h:213-215)
+    3-D fields  rho m1 m2 m3 e b1 b2 b3 eb rhob b1b b2b b3b (iotypes.h:217-219)
+
+Energies follow the synthetic-config convention e = p/(gamma-1) + rho v^2/2 +
+B^2/2 (the reference OT model divides B^2/2 by rho, models/init_user.cu.ot).
+Cell centres sit at xmin + (c - 2 + 1/2) dx for the blast wave and at
+(c - 2) dx for Orszag-Tang (so the periodic images of the ghosts are exact).
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass, field
+
+import numpy as np
+
+NG = 2  # ghost layers per side (ngi = 2, models/iosmaugparams.h.ot:1-3)
+
+
+def nvar(ndim: int) -> int:
+    return 4 + 3 * ndim
+
+
+def field_ids(ndim: int) -> dict:
+    D = ndim
+    ids = {"rho": 0, "e": 1 + D, "eb": 2 + 2 * D, "rhob": 3 + 2 * D}
+    for k in range(D):
+        ids[f"m{k+1}"] = 1 + k
+        ids[f"b{k+1}"] = 2 + D + k
+        ids[f"b{k+1}b"] = 4 + 2 * D + k
+    return ids
+
+
+@dataclass
+class Problem:
+    """A fully specified run: grid, physics constants and initial state."""
+
+    name: str
+    ndim: int
+    n: tuple            # cells per dim INCLUDING ghosts (x first)
+    dx: tuple           # uniform spacing per dim
+    xmin: tuple         # coordinate of cell 0 (a ghost) per dim
+    gamma: float
+    chyp: np.ndarray    # per field id
+    btype: tuple        # per dim: 0 periodic, 4 contcd4
+    courant: float
+    w: np.ndarray       # (NVAR, [n2,] n1, n0) float64
+    g: tuple = (0.0, 0.0, 0.0)
+    hyperdif: int = 1
+    meta: dict = field(default_factory=dict)
+
+    @property
+    def ncells(self) -> int:
+        return int(np.prod(self.n))
+
+    @property
+    def interior(self) -> int:
+        return int(np.prod([m - 2 * NG for m in self.n]))
+
+    def delx(self):
+        """Per-cell metric arrays (one per dim, grid-shaped), see metric()."""
+        return metric(self.n, self.xmin, self.dx)
+
+
+def metric(n, xmin, dx):
+    """Cell widths exactly as the reference derives them (initgrid,
+    init.cu:1118-1670): positions xmin + c*dx on every cell (init_parallel,
+    init.cu:128-140) go into a padded copy, every position component is
+    linearly extrapolated over the two outer layers of each direction in turn
+    (q(ix) = (1+|ixe-ix|) q(ixe) - |ixe-ix| q(ixf)), and
+    delx_d = (x_d[c+1] - x_d[c-1]) / 2 along d (0 replaced by dx).
+
+    Returns a list of ndim arrays shaped like one field ([k,] j, i).  Inside
+    the grid delx_d depends on the d coordinate only; the extrapolation
+    perturbs the last bits in the ghost layers of the other directions."""
+    D = len(n)
+    nn = list(n) + [1] * (3 - D)
+    shp = tuple(m + 2 for m in nn[:D]) + (1,) * (3 - D)   # (x, y, z) order
+    T = []
+    for d1 in range(D):
+        t = np.zeros(shp)
+        pos = xmin[d1] + np.arange(nn[d1]) * dx[d1]
+        sl = [slice(1, nn[e] + 1) if e < D else slice(0, 1) for e in range(3)]
+        view = [1, 1, 1]
+        view[d1] = nn[d1]
+        t[tuple(sl)] = pos.reshape(view)
+        T.append(t)
+    for d in range(D):
+        m = nn[d]
+        for (lo, hi, e, f) in ((m - 1, m + 1, m - 2, m - 3), (0, 2, 3, 4)):
+            for d1 in range(D):
+                t = np.moveaxis(T[d1], d, 0)
+                for ix in range(lo, hi + 1):
+                    a = abs(e - ix)
+                    t[ix] = (1 + a) * t[e] - a * t[f]
+    out = []
+    for d in range(D):
+        t = np.moveaxis(T[d], d, 0)
+        dd = 0.5 * (t[2:nn[d] + 2] - t[0:nn[d]])
+        dd = np.moveaxis(dd, 0, d)
+        inner = tuple(slice(1, nn[e] + 1) if (e < D and e != d) else slice(None) for e in range(3))
+        dd = dd[inner]
+        dd = np.where(dd == 0, dx[d], dd)
+        # (x, y, z) -> storage order ([z,] y, x)
+        dd = np.transpose(dd, (2, 1, 0))[(0,) if D == 2 else slice(None)]
+        out.append(np.ascontiguousarray(dd, dtype=np.float64))
+    return out
+
+
+def _chyp(ndim: int) -> np.ndarray:
+    """chyp values of models/iosmaugparams.h.ot:171-179 (sedov3d uses the same
+    per-kind values for its extra components)."""
+    ids = field_ids(ndim)
+    c = np.zeros(nvar(ndim))
+    c[ids["rho"]] = 0.045
+    c[ids["e"]] = 0.02
+    for k in range(ndim):
+        c[ids[f"m{k+1}"]] = 0.4
+        c[ids[f"b{k+1}"]] = 0.02
+    return c
+
+
+def orszag_tang(nx: int = 256, ny: int | None = None, b0_scale: float = 1.0,
+                rho_noise: float = 0.0, seed: int | None = None) -> Problem:
+    """2-D Orszag-Tang vortex on [0,1]^2, periodic, zero background fields."""
+    ny = nx if ny is None else ny
+    n = (nx + 2 * NG, ny + 2 * NG)
+    dx = (1.0 / nx, 1.0 / ny)
+    x = (np.arange(n[0]) - NG) * dx[0]
+    y = (np.arange(n[1]) - NG) * dx[1]
+    X, Y = np.meshgrid(x, y, indexing="xy")
+    gam = 5.0 / 3.0
+    rho = np.full(X.shape, 25.0 / (36.0 * np.pi))
+    if rho_noise:
+        rng = np.random.default_rng(seed)
+        inner = rho[NG:-NG, NG:-NG] * (1.0 + rho_noise * rng.standard_normal((ny, nx)))
+        rho[NG:-NG, NG:-NG] = inner
+        rho = _periodic_fill(rho)
+    p = 5.0 / (12.0 * np.pi)
+    B0 = b0_scale / np.sqrt(4.0 * np.pi)
+    vx = -np.sin(2 * np.pi * Y)
+    vy = np.sin(2 * np.pi * X)
+    bx = -B0 * np.sin(2 * np.pi * Y)
+    by = B0 * np.sin(4 * np.pi * X)
+    w = np.zeros((nvar(2),) + X.shape)
+    w[0] = rho
+    w[1] = rho * vx
+    w[2] = rho * vy
+    w[3] = p / (gam - 1) + 0.5 * rho * (vx * vx + vy * vy) + 0.5 * (bx * bx + by * by)
+    w[4] = bx
+    w[5] = by
+    w = np.stack([_periodic_fill(f) for f in w])
+    return Problem("orszag_tang", 2, n, dx, (-NG * dx[0], -NG * dx[1]), gam, _chyp(2), (0, 0),
+                   0.3, w, meta={"nx": nx, "ny": ny, "b0_scale": b0_scale, "rho_noise": rho_noise,
+                                 "seed": seed})
+
+
+def _periodic_fill(a: np.ndarray) -> np.ndarray:
+    out = a.copy()
+    for ax in range(a.ndim):
+        m = a.shape[ax]
+        idx = np.arange(m)
+        src = np.where(idx < NG, idx + m - 2 * NG, np.where(idx >= m - NG, idx - (m - 2 * NG), idx))
+        out = np.take(out, src, axis=ax)
+    return out
+
+
+def blast_wave(n: int = 128, seed: int = 1234) -> Problem:
+    """3-D blast wave on [-0.5, 0.5]^3, periodic: rho=1, p=0.1,
+    B=(1/sqrt2, 1/sqrt2, 0), p=10 inside r<0.1 about a centre jittered by
+    U(-dx/2, dx/2)^3 (PCG64 seeded)."""
+    N = (n + 2 * NG,) * 3
+    d = 1.0 / n
+    rng = np.random.default_rng(seed)
+    c0 = rng.uniform(-d / 2, d / 2, size=3)
+    ax = -0.5 + (np.arange(N[0]) - NG + 0.5) * d
+    Z, Y, X = np.meshgrid(ax, ax, ax, indexing="ij")  # arrays indexed [k, j, i]
+    r = np.sqrt((X - c0[0]) ** 2 + (Y - c0[1]) ** 2 + (Z - c0[2]) ** 2)
+    gam = 5.0 / 3.0
+    p = np.where(r < 0.1, 10.0, 0.1)
+    bx = by = 1.0 / np.sqrt(2.0)
+    w = np.zeros((nvar(3),) + X.shape)
+    w[0] = 1.0
+    w[4] = p / (gam - 1) + 0.5 * (bx * bx + by * by)
+    w[5] = bx
+    w[6] = by
+    w = np.stack([_periodic_fill(f) for f in w])
+    return Problem("blast_wave", 3, N, (d, d, d), (-0.5 - (NG - 0.5) * d,) * 3, gam, _chyp(3),
+                   (0, 0, 0), 0.3, w, meta={"n": n, "seed": seed, "centre": c0.tolist()})
