@@ -1,0 +1,128 @@
+/*
+ * smaug_b200.h -- C ABI of the B200 ideal-MHD step (SAC/SMAUG method).
+ *
+ * The reference drives its GPU step through ~35 per-operator entry points
+ * declared in dev/smaug/include/smaugcukernels.h (cuinit, cucentdiff1,
+ * cuhyperdifvisc1r, cuboundary, ...), called in sequence by the host loop
+ * dev/smaug/src/iosmaug.cpp:802-1550.  This library exposes the same step at
+ * the granularity a host loop needs, with plain pointers and sizes only:
+ *
+ *   smaug_create        replaces cuinit            (init.cu:816-1000)
+ *   smaug_set_metric    replaces initgrid          (init.cu:1118-1670)
+ *   smaug_set_state     replaces cuinit's H2D copy + the initial cuboundary
+ *                       pass                       (iosmaug.cpp:786-794)
+ *   smaug_step          replaces one loop iteration: cucomputedervfields,
+ *                       the moddton dt block (cucomputec / cucomputemaxc /
+ *                       cucomputemaxcourant / cugetdtvisc1), cucentdiff1/2,
+ *                       cugrav, the hyperdiffusion chains (cuhyperdifvisc1r/l
+ *                       + cuhyperdif*source*), cusource and cuboundary
+ *                                                  (iosmaug.cpp:802-1166)
+ *   smaug_get_state     replaces cuupdate          (update.cu:162-235)
+ *   smaug_get_scalars   replaces reading p->dt, p->cmax, p->maxcourant,
+ *                       p->maxviscoef, p->dtdiffvisc back from struct params
+ *   smaug_destroy       replaces cufinish          (init.cu, never called by
+ *                       the reference)
+ *
+ * Storage (same as the reference's wmod slot, iotypes.h:213-219): host state
+ * buffers hold NVAR fields, field-major, x fastest, each of N cells
+ * including two ghost layers per side:
+ *   2-D: rho m1 m2 e b1 b2 eb rhob b1b b2b              NVAR = 10
+ *   3-D: rho m1 m2 m3 e b1 b2 b3 eb rhob b1b b2b b3b    NVAR = 13
+ *
+ * Errors: every function returns SMAUG_OK (0) or a negative status and never
+ * aborts (the reference's int-returning wrappers have no return value at
+ * all); smaug_last_error() describes the last failure.  All work of one
+ * context is ordered on one CUDA stream; one host thread per context.
+ */
+#ifndef SMAUG_B200_H
+#define SMAUG_B200_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+  SMAUG_OK = 0,
+  SMAUG_ERR_ARG = -1,      /* invalid argument or size */
+  SMAUG_ERR_CUDA = -2,     /* CUDA runtime error */
+  SMAUG_ERR_STATE = -3,    /* call out of order (e.g. step before set_state) */
+  SMAUG_ERR_NONFINITE = -4 /* dt or a reduction became NaN/Inf */
+};
+
+/* Boundary types per direction (iotypes.h:145 boundtype codes). */
+enum { SMAUG_BC_PERIODIC = 0, SMAUG_BC_CONTCD4 = 4 };
+
+typedef struct smaug_ctx smaug_ctx;
+
+typedef struct {
+  int ndim;         /* 2 or 3 */
+  int n[3];         /* cells per dim INCLUDING 2+2 ghost layers (n[2] = 1 in 2-D) */
+  double gamma;     /* p->gamma */
+  double courant;   /* p->courant */
+  double chyp[13];  /* p->chyp, indexed by field id (layout above) */
+  int btype[3];     /* per dim, SMAUG_BC_*; same for every field and both sides */
+  double g[3];      /* p->g */
+  int hyperdif;     /* p->hyperdifmom: 1 = hyperdiffusion sources on */
+  int rk4;          /* 1: classical four-stage RK (SAC fourstep); 0: single step (rkon=0) */
+  int dt_mode;      /* 1: dt from the reference's moddton rule; 0: fixed dt = dt0 */
+  double dt0;       /* initial dt (1e-8 when dt_mode = 1, iosmaug.cpp:327-330) */
+  int exact;        /* 1: kernels built without FMA contraction (bit-reproducible) */
+} smaug_params;
+
+/* Number of fields for ndim (10 or 13). */
+int smaug_nvar(int ndim);
+
+int smaug_create(const smaug_params *prm, int device, smaug_ctx **out);
+int smaug_destroy(smaug_ctx *ctx);
+
+/*
+ * Metric: ndim arrays of N doubles (cell widths along each dim at every cell,
+ * the reference's wd[delx1..delx3] after initgrid), concatenated.
+ */
+int smaug_set_metric(smaug_ctx *ctx, const double *delx, size_t count);
+
+/* Host state in/out: NVAR * N doubles (layout above).  Synchronous. */
+int smaug_set_state(smaug_ctx *ctx, const double *w, size_t count);
+int smaug_get_state(smaug_ctx *ctx, double *w, size_t count);
+
+/* Device-resident variants: w points to NVAR * N doubles in device memory;
+ * the copy is ordered on the context stream and not waited for. */
+int smaug_set_state_device(smaug_ctx *ctx, const double *w_dev, size_t count);
+int smaug_get_state_device(smaug_ctx *ctx, double *w_dev, size_t count);
+
+/* Advance nsteps full steps (asynchronous on the context stream). */
+int smaug_step(smaug_ctx *ctx, int nsteps);
+
+/* Wait for all queued work; returns the first device-side error if any. */
+int smaug_sync(smaug_ctx *ctx);
+
+/*
+ * out[0] dt of the last step, [1] maxcourant, [2] maxviscoef (running),
+ * [3] dtdiffvisc, [4..6] cmax per dim of the current state,
+ * [7] steps taken.  Synchronous.
+ */
+int smaug_get_scalars(smaug_ctx *ctx, double out[8]);
+
+/*
+ * Stage timing: when enabled, CUDA events bracket every stage kernel launch;
+ * smaug_stage_times waits, returns the summed device time (ms) and the number
+ * of timed launches since the last call, and resets.  (The reference's only
+ * timing is the per-step wall clock printf, iosmaug.cpp:1515-1517.)
+ */
+int smaug_profile_stages(smaug_ctx *ctx, int enable);
+int smaug_stage_times(smaug_ctx *ctx, double *ms_total, long long *count);
+
+/* The CUDA stream (cudaStream_t) all work of ctx is ordered on. */
+void *smaug_stream(smaug_ctx *ctx);
+
+/* Kernel launches issued so far by ctx (for launch accounting). */
+long long smaug_launch_count(smaug_ctx *ctx);
+
+const char *smaug_last_error(smaug_ctx *ctx);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,74 @@
+"""Build the CUDA library in-tree: smaug-all_b200/lib/libsmaug_b200.so.
+
+nvcc cross-compiles for sm_100a (B200) on a machine without a GPU.  The stage
+kernels are compiled twice: stage_exact.cu with -fmad=false (bit-reproducible
+against the CPU oracle) and stage_fast.cu with FMA contraction.
+"""
+from __future__ import annotations
+
+import os
+import subprocess
+import sys
+from concurrent.futures import ThreadPoolExecutor
+from pathlib import Path
+
+PKG = Path(__file__).resolve().parents[2]          # smaug-all_b200/
+CSRC = PKG / "csrc"
+LIBDIR = PKG / "lib"
+LIB = LIBDIR / "libsmaug_b200.so"
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+NVCC = os.environ.get("NVCC", "nvcc")
+COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC,-O2", "--expt-relaxed-constexpr"] + ARCH
+
+UNITS = [
+    ("stage_exact.cu", ["-fmad=false"]),
+    ("stage_fast.cu", ["-fmad=true"]),
+    ("smaug_capi.cu", []),
+]
+
+
+def sources():
+    return sorted(CSRC.glob("*.cu")) + sorted(CSRC.glob("*.cuh")) + sorted(CSRC.glob("*.inc")) + [
+        PKG.parent / "include" / "smaug_b200.h"]
+
+
+def up_to_date() -> bool:
+    if not LIB.exists():
+        return False
+    t = LIB.stat().st_mtime
+    return all(s.stat().st_mtime <= t for s in sources())
+
+
+def build(force: bool = False, verbose: bool = False) -> Path:
+    if not force and up_to_date():
+        return LIB
+    LIBDIR.mkdir(parents=True, exist_ok=True)
+    objdir = LIBDIR / "obj"
+    objdir.mkdir(exist_ok=True)
+
+    def one(unit):
+        src, extra = unit
+        obj = objdir / (Path(src).stem + ".o")
+        cmd = [NVCC, *COMMON, *extra, "-Xptxas", "-v", "-c", str(CSRC / src), "-o", str(obj)]
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError(f"nvcc failed for {src}:\n{' '.join(cmd)}\n{r.stderr[-6000:]}")
+        (objdir / (Path(src).stem + ".ptxas.txt")).write_text(r.stderr)
+        if verbose:
+            print(r.stderr)
+        return obj
+
+    with ThreadPoolExecutor(max_workers=len(UNITS)) as ex:
+        objs = list(ex.map(one, UNITS))
+    tmp = LIB.with_suffix(".so.tmp")
+    cmd = [NVCC, "-shared", *ARCH, "-o", str(tmp), *map(str, objs), "-lcudart"]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"link failed:\n{r.stderr[-4000:]}")
+    os.replace(tmp, LIB)
+    return LIB
+
+
+if __name__ == "__main__":
+    build(force="--force" in sys.argv, verbose="-v" in sys.argv)
+    print(LIB)

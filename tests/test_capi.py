@@ -1,0 +1,59 @@
+"""The C ABI library builds, loads and exports every entry point declared in
+include/smaug_b200.h (no device work: these run without a GPU)."""
+from __future__ import annotations
+
+import ctypes
+import re
+from pathlib import Path
+
+import pytest
+
+from smaug_b200 import LIB_PATH, load_library
+
+ROOT = Path(__file__).resolve().parents[1]
+HEADER = ROOT / "include" / "smaug_b200.h"
+
+
+def declared_functions():
+    text = HEADER.read_text()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(smaug_\w+)\s*\(", text)))
+
+
+def test_header_declares_entry_points():
+    names = declared_functions()
+    for must in ["smaug_create", "smaug_destroy", "smaug_set_metric", "smaug_set_state", "smaug_get_state",
+                 "smaug_step", "smaug_sync", "smaug_get_scalars", "smaug_last_error"]:
+        assert must in names
+
+
+def test_library_exports_every_declared_symbol():
+    assert LIB_PATH.exists(), "libsmaug_b200.so not built"
+    lib = ctypes.CDLL(str(LIB_PATH))
+    missing = [n for n in declared_functions() if not hasattr(lib, n)]
+    assert not missing, missing
+
+
+def test_pure_host_entry_points():
+    lib = load_library()
+    assert lib.smaug_nvar(2) == 10 and lib.smaug_nvar(3) == 13
+    lib.smaug_last_error.restype = ctypes.c_char_p
+    assert lib.smaug_last_error(None) == b"null context"
+    assert lib.smaug_destroy(None) == 0
+
+
+def test_create_rejects_bad_arguments():
+    from smaug_b200 import Params
+    lib = load_library()
+    p = Params()
+    p.ndim = 4
+    h = ctypes.c_void_p()
+    rc = lib.smaug_create(ctypes.byref(p), 0, ctypes.byref(h))
+    assert rc == -1
+    assert b"ndim" in lib.smaug_last_error(h)
+    lib.smaug_destroy(h)
+    p.ndim = 2
+    p.n[0], p.n[1] = 8, 40
+    h = ctypes.c_void_p()
+    assert lib.smaug_create(ctypes.byref(p), 0, ctypes.byref(h)) == -1
+    lib.smaug_destroy(h)

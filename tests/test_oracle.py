@@ -1,0 +1,104 @@
+"""The oracle (our CPU restatement) against the reference.
+
+* golden fixtures made by the reference's own code (tests/golden/make_golden.py)
+  must be reproduced bit for bit;
+* where the host build of the reference is present (oracle/_ref, built in the
+  build container), it is also run live on fresh cases.
+"""
+from __future__ import annotations
+
+import json
+import subprocess
+import sys
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from smaug_b200 import problems
+
+ROOT = Path(__file__).resolve().parents[1]
+GOLD = ROOT / "tests" / "golden"
+sys.path.insert(0, str(GOLD))
+from make_golden import CASES, make_problem  # noqa: E402
+
+from oracle.oracle import Oracle  # noqa: E402
+
+REF_LIBS = [ROOT / "oracle" / "_ref" / f"libsmaug_ref{d}d.so" for d in (2, 3)]
+
+
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_oracle_reproduces_golden(name):
+    spec = json.loads((GOLD / f"{name}.json").read_text())["spec"]
+    gold = np.load(GOLD / f"{name}.npz")
+    prob = make_problem(spec)
+    o = Oracle(prob)
+    dts = []
+    for _ in range(spec["steps"]):
+        o.step(1, rk4=spec["rk4"])
+        dts.append(o.dt)
+    assert np.array_equal(np.array(dts), gold["dts"]), (dts, gold["dts"])
+    assert np.array_equal(o.w, gold["w_final"])
+
+
+def _run_ref_vs_oracle(kind, n, btype, steps):
+    code = f"""
+import sys, numpy as np
+sys.path.insert(0, {str(ROOT)!r}); sys.path.insert(0, {str(ROOT / 'smaug-all_b200' / 'python')!r})
+from smaug_b200 import problems
+from oracle.oracle import Oracle, Reference
+prob = problems.orszag_tang({n}) if {kind!r} == 'ot' else problems.blast_wave({n}, seed=7)
+if {btype!r}: prob.btype = tuple({btype!r})
+r = Reference(prob); o = Oracle(prob)
+for s in range({steps}):
+    wr = r.step(1); wo = o.step(1, rk4=False)
+    assert r.dt == o.dt, (s, r.dt, o.dt)
+    assert np.array_equal(wr, wo), (s, float(np.max(np.abs(wr - wo))))
+print('OK')
+"""
+    res = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, timeout=600)
+    assert res.returncode == 0 and "OK" in res.stdout, res.stderr[-3000:] + res.stdout[-2000:]
+
+
+@pytest.mark.skipif(not all(p.exists() for p in REF_LIBS), reason="host build of the reference not present")
+@pytest.mark.parametrize("kind,n,btype,steps", [
+    ("ot", 32, None, 10), ("ot", 28, [4, 4], 6), ("blast", 12, None, 5), ("blast", 12, [0, 4, 0], 4),
+])
+def test_oracle_bit_exact_vs_reference_live(kind, n, btype, steps):
+    _run_ref_vs_oracle(kind, n, btype, steps)
+
+
+def test_metric_is_tensor_product_inside():
+    prob = problems.blast_wave(12)
+    for d, m in enumerate(prob.delx()):
+        inner = m[2:-2, 2:-2, 2:-2]
+        line = np.moveaxis(inner, 2 - d, 0)
+        assert np.all(line == line[:, :1, :1])
+
+
+def test_rk4_is_fourstep_of_single_step_operator():
+    """RK4 stage = base + h L(in); with base = in it equals one single step."""
+    prob = problems.orszag_tang(16)
+    o = Oracle(prob)
+    w = o.w.copy()
+    cm = o.cmax(w)
+    a, _ = o.stage(w, w, 1e-3, cm)
+    o2 = Oracle(prob, dt_fixed=1e-3)
+    o2.step(1, rk4=False, dt_mode=0)
+    assert np.array_equal(a, o2.w)
+
+
+def test_boundary_fill_periodic_and_contcd4():
+    prob = problems.orszag_tang(12)
+    prob.btype = (0, 4)
+    o = Oracle(prob)
+    rng = np.random.default_rng(0)
+    w = rng.standard_normal(prob.w.shape)
+    f = o.boundary(w)
+    n0 = prob.n[0]
+    assert np.array_equal(f[:6, :, 0], f[:6, :, n0 - 4])
+    assert np.array_equal(f[:6, :, n0 - 1], f[:6, :, 3])
+    assert np.array_equal(f[:6, 0, :], f[:6, 4, :])
+    assert np.array_equal(f[:6, 1, :], f[:6, 3, :])
+    assert np.array_equal(f[:6, -1, :], f[:6, -5, :])
+    assert np.array_equal(f[6:], w[6:])  # backgrounds untouched
