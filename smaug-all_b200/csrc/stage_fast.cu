@@ -1,3 +1,5 @@
-// Stage kernels built with FMA contraction (the production FP64 variant).
+// Production stage kernels: the shared-memory tiled kernel, built with FMA
+// contraction.
 #define SMAUG_NS smaug_fast
+#define SMAUG_TILED 1
 #include "stage_variant.inc"
