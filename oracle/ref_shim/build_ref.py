@@ -18,13 +18,13 @@ Recipe (our own; the reference Makefile is not run):
    its own cell).  The four shared-memory max reductions are replaced by
    ``shim_blockmax`` with identical block maxima.
 3. Three source patches, each a documented deviation of the pin:
-   P1 hyperdifvisc1r.cu:1236/1264 -- ``hyperdifvisc1r_parallel`` stores q through
+   P1 hyperdifvisc1r.cu:1235,1253 -- ``hyperdifvisc1r_parallel`` stores q through
       the unpadded encoder ``encode3`` into the padded array wtemp2 while other
       threads zero that array in the same launch (a data race whose only
       surviving effect is garbage in the right-hand pad column).  Patched to
       ``encode3p2``; the value is then rewritten by hyperdifvisc1ar anyway and
       the pad column keeps the 0 that the zeroing pass writes.
-   P2 computedervfields.cu:1355 -- ``temp[index]=0.0`` with ``index``
+   P2 computedervfields.cu:1353 -- ``temp[index]=0.0`` with ``index``
       uninitialised (undefined behaviour) becomes ``temp[iindex]=0.0``; those
       entries are already 0 at that point.
    P3 boundary.cu -- models/boundary.cu.sedov3d (periodic, contcd4 and fixed

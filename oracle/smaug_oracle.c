@@ -634,7 +634,7 @@ int sm_oracle_step(const sm_oracle_grid *g, double *w, int step, int rk4, int dt
     sm_oracle_boundary(g, w);
   }
   /* The reference resets p->maxviscoef at the start of its hyperdiffusion
-   * block (iosmaug.cpp:972), but the next call, cucomputec
+   * block (iosmaug.cpp:973), but the next call, cucomputec
    * (computedervfields.cu:2298-2328), copies the device params back over the
    * host copy, restoring the previous value: the coefficient is a running
    * maximum over all steps. */

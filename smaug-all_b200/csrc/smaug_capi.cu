@@ -5,7 +5,7 @@
 //   dt_kernel                 the reference's moddton dt block
 //                             (iosmaug.cpp:855-898), from maxima that the
 //                             previous stage already reduced on the device
-//   stage_kernel x 4 (or 1)   fused RK stages (fluxes + hyperdiffusion +
+//   stage kernel x 4 (or 1)   fused RK stages (fluxes + hyperdiffusion +
 //                             ghost fill + wave-speed maxima)
 //   finish_kernel             running maxviscoef, carry the maxima
 // No host round trip happens inside a step (the reference copies struct
@@ -35,41 +35,26 @@ void launch_reduce(int D, const double *w, const double *bg, const smaug::Geo &g
 
 using namespace smaug;
 
-struct smaug_ctx {
-  smaug_params prm;
-  int device = 0;
+namespace {
+
+// Everything one simulation's launches need: the context API and the
+// no-allocation entry point both fill one of these.
+struct Run {
   int D = 0, NW = 0, NB = 0, NVAR = 0;
   Geo geo{};
   Phys phys{};
+  bool rk4 = true, exact = false;
+  double dt0 = 0.0;
   cudaStream_t stream = nullptr;
-  double *W[4] = {nullptr, nullptr, nullptr, nullptr};  // state, RK stages / ping-pong
+  double *W[4] = {nullptr, nullptr, nullptr, nullptr};  // state, then RK stages (or ping-pong)
   double *bg = nullptr;
-  double *dx1 = nullptr;     // concatenated 1-D metric
-  double *dxlast = nullptr;  // full metric of the last dim
   DevScalars *sc = nullptr;
-  bool have_metric = false, have_state = false;
-  int cur = 0;  // which W buffer holds the state (single-step ping-pong)
+  int cur = 0;
   long long launches = 0;
-  long long steps = 0;
-  std::string err;
-  // optional per-stage timing (the reference's tcal accumulator, iosmaug.cpp:1515-1517)
-  bool profile = false;
-  std::vector<cudaEvent_t> ev;  // pairs around stage launches
-  size_t ev_used = 0;
+  // optional per-stage timing
+  std::vector<cudaEvent_t> *ev = nullptr;
+  size_t *ev_used = nullptr;
 };
-
-namespace {
-
-int fail(smaug_ctx *c, int code, const std::string &m) {
-  if (c) c->err = m;
-  return code;
-}
-
-#define CK(call)                                                                             \
-  do {                                                                                       \
-    cudaError_t e_ = (call);                                                                 \
-    if (e_ != cudaSuccess) return fail(ctx, SMAUG_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
-  } while (0)
 
 // ndimp of the reference's reductions (computedervfields.cu:1940-1950).
 long long ref_ndimp(long long dimp) {
@@ -83,8 +68,50 @@ long long ref_ndimp(long long dimp) {
   return dimp;
 }
 
+// Validate params and fill the size/physics part of a Run.  Returns an error
+// message or nullptr.
+const char *plan(const smaug_params *prm, Run &r) {
+  const int D = prm->ndim;
+  if (D != 2 && D != 3) return "ndim must be 2 or 3";
+  r.D = D;
+  r.NW = 2 + 2 * D;
+  r.NVAR = 4 + 3 * D;
+  r.NB = r.NVAR - r.NW;
+  long long N = 1;
+  for (int d = 0; d < 3; ++d) {
+    const int n = d < D ? prm->n[d] : 1;
+    if (d < D && (n < 10 || n > (1 << 20))) return "each dimension needs 10..2^20 cells including ghosts";
+    if (d < D && prm->btype[d] != SMAUG_BC_PERIODIC && prm->btype[d] != SMAUG_BC_CONTCD4)
+      return "boundary type must be periodic (0) or contcd4 (4)";
+    r.geo.n[d] = n;
+    r.geo.btype[d] = d < D ? prm->btype[d] : 0;
+    N *= n;
+  }
+  r.geo.st[0] = 1;
+  r.geo.st[1] = r.geo.n[0];
+  r.geo.st[2] = (long long)r.geo.n[0] * r.geo.n[1];
+  r.geo.N = N;
+  r.geo.K = ((ref_ndimp(N) + 511) / 512) * 64;
+  Phys &p = r.phys;
+  p.gamma = prm->gamma;
+  p.courant = prm->courant;
+  for (int f = 0; f < 13; ++f) p.chyp[f] = prm->chyp[f];
+  p.has_grav = 0;
+  for (int d = 0; d < 3; ++d) {
+    p.g[d] = d < D ? prm->g[d] : 0.0;
+    if (p.g[d] != 0.0) p.has_grav = 1;
+  }
+  p.hyperdif = prm->hyperdif;
+  p.dt_mode = prm->dt_mode;
+  p.has_bgb = 1;
+  r.rk4 = prm->rk4 != 0;
+  r.exact = prm->exact != 0;
+  r.dt0 = prm->dt0;
+  return nullptr;
+}
+
 // Ghost fill of the evolved fields from their interior sources (periodic /
-// contcd4), used once when a state is loaded (iosmaug.cpp:786-794).
+// contcd4), used when a state is loaded (iosmaug.cpp:786-794).
 __global__ void ghost_fill_kernel(double *w, int nw, Geo g, int D) {
   for (long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x; j < g.N; j += (long long)gridDim.x * blockDim.x) {
     long long r = j;
@@ -128,7 +155,7 @@ __global__ void dt_kernel(DevScalars *sc, Phys p, int D) {
       double dtd = 0.0000000001;
       for (int dir = 0; dir < D; ++dir) {
         double m = cpred;
-        double v = ((sc->maxviscoef) + 0.0) / (p.minsq[dir]);
+        double v = ((sc->maxviscoef) + 0.0) / (sc->minsq[dir]);
         if (v > m) m = v;
         if (m > dtd) dtd = m;
         dtd = 0.25 / dtd;
@@ -157,28 +184,159 @@ __global__ void finish_kernel(DevScalars *sc, int last) {
   }
 }
 
-void launch_stage(smaug_ctx *c, const StageArgs &a) {
-  cudaEvent_t e0 = nullptr, e1 = nullptr;
-  if (c->profile) {
-    while (c->ev.size() < c->ev_used + 2) {
+// Fresh run state: dt0, counters and maxima cleared (minsq kept: it belongs
+// to the metric).
+__global__ void reset_scalars_kernel(DevScalars *sc, double dt0) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  sc->dt = dt0;
+  sc->dtdiffvisc = 0.0;
+  sc->maxviscoef = 0.0;
+  sc->maxcourant = 0.0;
+  sc->step = 0;
+  sc->status = 0;
+  for (int s = 0; s < 5; ++s)
+    for (int k = 0; k < 8; ++k) sc->red[s].v[k] = 0ull;
+}
+
+void launch_stage(Run &r, const StageArgs &a) {
+  cudaEvent_t e1 = nullptr;
+  if (r.ev && r.ev_used) {
+    while (r.ev->size() < *r.ev_used + 2) {
       cudaEvent_t e;
       if (cudaEventCreate(&e) != cudaSuccess) break;
-      c->ev.push_back(e);
+      r.ev->push_back(e);
     }
-    if (c->ev.size() >= c->ev_used + 2) {
-      e0 = c->ev[c->ev_used];
-      e1 = c->ev[c->ev_used + 1];
-      c->ev_used += 2;
-      cudaEventRecord(e0, c->stream);
+    if (r.ev->size() >= *r.ev_used + 2) {
+      cudaEventRecord((*r.ev)[*r.ev_used], r.stream);
+      e1 = (*r.ev)[*r.ev_used + 1];
+      *r.ev_used += 2;
     }
   }
-  if (c->prm.exact)
-    smaug_exact::launch_stage(c->D, a, c->geo, c->phys, c->stream);
+  if (r.exact)
+    smaug_exact::launch_stage(r.D, a, r.geo, r.phys, r.stream);
   else
-    smaug_fast::launch_stage(c->D, a, c->geo, c->phys, c->stream);
-  if (e1) cudaEventRecord(e1, c->stream);
-  c->launches++;
+    smaug_fast::launch_stage(r.D, a, r.geo, r.phys, r.stream);
+  if (e1) cudaEventRecord(e1, r.stream);
+  r.launches++;
 }
+
+// A state is in r.W[0] (evolved) and r.bg: fill ghosts, reset scalars,
+// reduce the initial maxima.  Asynchronous.
+cudaError_t run_load(Run &r) {
+  r.cur = 0;
+  ghost_fill_kernel<<<148 * 8, 256, 0, r.stream>>>(r.W[0], r.NW, r.geo, r.D);
+  const double dt0 = r.phys.dt_mode == 1 ? (r.dt0 > 0 ? r.dt0 : 1.0e-8) : r.dt0;
+  reset_scalars_kernel<<<1, 1, 0, r.stream>>>(r.sc, dt0);
+  if (r.exact)
+    smaug_exact::launch_reduce(r.D, r.W[0], r.bg, r.geo, r.phys, &r.sc->red[0], r.stream);
+  else
+    smaug_fast::launch_reduce(r.D, r.W[0], r.bg, r.geo, r.phys, &r.sc->red[0], r.stream);
+  r.launches += 3;
+  return cudaGetLastError();
+}
+
+// Enqueue nsteps full steps.
+cudaError_t run_steps(Run &r, int nsteps) {
+  for (int it = 0; it < nsteps; ++it) {
+    dt_kernel<<<1, 1, 0, r.stream>>>(r.sc, r.phys, r.D);
+    r.launches++;
+    StageArgs a{};
+    a.bg = r.bg;
+    a.sc = r.sc;
+    if (!r.rk4) {
+      double *w = r.W[r.cur], *o = r.W[1 - r.cur];
+      a.in = w; a.base = w; a.out = o; a.acc = nullptr; a.kind = 0;
+      a.red_in = 0; a.red_out = 1; a.hdiv = 1.0;
+      launch_stage(r, a);
+      finish_kernel<<<1, 1, 0, r.stream>>>(r.sc, 1);
+      r.cur = 1 - r.cur;
+    } else {
+      // SAC fourstep (vac.t:447-462): W1 = W + dt/2 L(W); W2 = W + dt/2 L(W1);
+      // W3 = W + dt L(W2) and W1 <- (W1 + 2 W2 + W3 - 4 W)/3; W <- (W + dt/6 L(W3)) + W1
+      double *W = r.W[0], *W1 = r.W[1], *W2 = r.W[2], *W3 = r.W[3];
+      a.base = W;
+      a.in = W;  a.out = W1; a.acc = nullptr; a.kind = 0; a.red_in = 0; a.red_out = 1; a.hdiv = 2.0;
+      launch_stage(r, a);
+      a.in = W1; a.out = W2; a.red_in = 1; a.red_out = 2; a.hdiv = 2.0;
+      launch_stage(r, a);
+      a.in = W2; a.out = W3; a.acc = W1; a.kind = 3; a.red_in = 2; a.red_out = 3; a.hdiv = 1.0;
+      launch_stage(r, a);
+      a.in = W3; a.out = W;  a.acc = W1; a.kind = 4; a.red_in = 3; a.red_out = 4; a.hdiv = 6.0;
+      launch_stage(r, a);
+      finish_kernel<<<1, 1, 0, r.stream>>>(r.sc, 4);
+    }
+    r.launches++;
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
+}
+
+// 1-D metric lines, tensor-product check and min delx^2 over the first K
+// cells, from a host metric (ndim * N doubles).  Returns an error or nullptr.
+const char *metric_host(const Run &r, const double *delx, double *d1, double minsq[3]) {
+  const int D = r.D;
+  const long long N = r.geo.N;
+  size_t off = 0;
+  for (int d = 0; d < 3; ++d) minsq[d] = INFINITY;
+  for (int d = 0; d < D; ++d) {
+    const double *m = delx + (size_t)d * N;
+    const int n = r.geo.n[d];
+    for (int x = 0; x < n; ++x) {
+      int c[3] = {2, 2, D == 3 ? 2 : 0};
+      c[d] = x;
+      d1[off + x] = m[c[0] + c[1] * r.geo.st[1] + c[2] * r.geo.st[2]];
+    }
+    for (long long j = 0; j < N; ++j) {
+      long long q = j;
+      int c[3];
+      c[0] = (int)(q % r.geo.n[0]);
+      q /= r.geo.n[0];
+      c[1] = (int)(q % r.geo.n[1]);
+      c[2] = (int)(q / r.geo.n[1]);
+      bool inner = true;
+      for (int e = 0; e < D; ++e)
+        if (c[e] < 2 || c[e] > r.geo.n[e] - 3) inner = false;
+      if (inner && m[j] != d1[off + c[d]]) return "metric is not a tensor-product grid on the inner cells";
+      if (!(m[j] > 0.0)) return "metric entries must be positive";
+      if (j < r.geo.K) {
+        const double v = (m[j]) * (m[j]);
+        if (v < minsq[d]) minsq[d] = v;
+      }
+    }
+    off += n;
+  }
+  return nullptr;
+}
+
+}  // namespace
+
+struct smaug_ctx {
+  smaug_params prm;
+  int device = 0;
+  Run run;
+  double *dx1 = nullptr;     // concatenated 1-D metric
+  double *dxlast = nullptr;  // full metric of the last dim
+  bool have_metric = false, have_state = false;
+  long long steps = 0;
+  std::string err;
+  bool profile = false;
+  std::vector<cudaEvent_t> ev;
+  size_t ev_used = 0;
+};
+
+namespace {
+
+int fail(smaug_ctx *c, int code, const std::string &m) {
+  if (c) c->err = m;
+  return code;
+}
+
+#define CK(call)                                                                             \
+  do {                                                                                       \
+    cudaError_t e_ = (call);                                                                 \
+    if (e_ != cudaSuccess) return fail(ctx, SMAUG_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+  } while (0)
 
 }  // namespace
 
@@ -192,173 +350,91 @@ int smaug_create(const smaug_params *prm, int device, smaug_ctx **out) {
   smaug_ctx *ctx = new smaug_ctx();
   ctx->prm = *prm;
   ctx->device = device;
-  const int D = prm->ndim;
-  if (D != 2 && D != 3) {
-    int r = fail(ctx, SMAUG_ERR_ARG, "ndim must be 2 or 3");
-    *out = ctx;
-    return r;
-  }
-  ctx->D = D;
-  ctx->NW = 2 + 2 * D;
-  ctx->NVAR = 4 + 3 * D;
-  ctx->NB = ctx->NVAR - ctx->NW;
-  long long N = 1;
-  for (int d = 0; d < 3; ++d) {
-    int n = d < D ? prm->n[d] : 1;
-    if (d < D && (n < 10 || n > (1 << 20))) {
-      int r = fail(ctx, SMAUG_ERR_ARG, "each dimension needs 10..2^20 cells including ghosts");
-      *out = ctx;
-      return r;
-    }
-    if (d < D && prm->btype[d] != SMAUG_BC_PERIODIC && prm->btype[d] != SMAUG_BC_CONTCD4) {
-      int r = fail(ctx, SMAUG_ERR_ARG, "boundary type must be periodic (0) or contcd4 (4)");
-      *out = ctx;
-      return r;
-    }
-    ctx->geo.n[d] = n;
-    ctx->geo.btype[d] = d < D ? prm->btype[d] : 0;
-    N *= n;
-  }
-  ctx->geo.st[0] = 1;
-  ctx->geo.st[1] = ctx->geo.n[0];
-  ctx->geo.st[2] = (long long)ctx->geo.n[0] * ctx->geo.n[1];
-  ctx->geo.N = N;
-  const long long ndimp = ref_ndimp(N);
-  ctx->geo.K = ((ndimp + 511) / 512) * 64;
-  Phys &p = ctx->phys;
-  p.gamma = prm->gamma;
-  p.courant = prm->courant;
-  for (int f = 0; f < 13; ++f) p.chyp[f] = prm->chyp[f];
-  p.has_grav = 0;
-  for (int d = 0; d < 3; ++d) {
-    p.g[d] = d < D ? prm->g[d] : 0.0;
-    if (p.g[d] != 0.0) p.has_grav = 1;
-  }
-  p.hyperdif = prm->hyperdif;
-  p.dt_mode = prm->dt_mode;
   *out = ctx;
+  Run &r = ctx->run;
+  if (const char *m = plan(prm, r)) return fail(ctx, SMAUG_ERR_ARG, m);
+  r.ev = &ctx->ev;
   CK(cudaSetDevice(device));
-  CK(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
-  const size_t fsz = sizeof(double) * (size_t)N;
-  const int nbuf = 4;
-  for (int b = 0; b < nbuf; ++b) CK(cudaMalloc(&ctx->W[b], fsz * ctx->NW));
-  CK(cudaMalloc(&ctx->bg, fsz * ctx->NB));
-  CK(cudaMalloc(&ctx->dx1, sizeof(double) * (ctx->geo.n[0] + ctx->geo.n[1] + ctx->geo.n[2])));
+  CK(cudaStreamCreateWithFlags(&r.stream, cudaStreamNonBlocking));
+  const size_t fsz = sizeof(double) * (size_t)r.geo.N;
+  for (int b = 0; b < 4; ++b) CK(cudaMalloc(&r.W[b], fsz * r.NW));
+  CK(cudaMalloc(&r.bg, fsz * r.NB));
+  CK(cudaMalloc(&ctx->dx1, sizeof(double) * (r.geo.n[0] + r.geo.n[1] + r.geo.n[2])));
   CK(cudaMalloc(&ctx->dxlast, fsz));
-  CK(cudaMalloc(&ctx->sc, sizeof(DevScalars)));
-  CK(cudaMemsetAsync(ctx->sc, 0, sizeof(DevScalars), ctx->stream));
-  CK(cudaStreamSynchronize(ctx->stream));
+  CK(cudaMalloc(&r.sc, sizeof(DevScalars)));
+  CK(cudaMemsetAsync(r.sc, 0, sizeof(DevScalars), r.stream));
+  CK(cudaStreamSynchronize(r.stream));
   return SMAUG_OK;
 }
 
 int smaug_destroy(smaug_ctx *ctx) {
   if (!ctx) return SMAUG_OK;
+  Run &r = ctx->run;
   cudaSetDevice(ctx->device);
-  if (ctx->stream) cudaStreamSynchronize(ctx->stream);
-  for (auto &b : ctx->W) cudaFree(b);
-  cudaFree(ctx->bg);
+  if (r.stream) cudaStreamSynchronize(r.stream);
+  for (auto &b : r.W) cudaFree(b);
+  cudaFree(r.bg);
   cudaFree(ctx->dx1);
   cudaFree(ctx->dxlast);
-  cudaFree(ctx->sc);
+  cudaFree(r.sc);
   for (auto e : ctx->ev) cudaEventDestroy(e);
-  if (ctx->stream) cudaStreamDestroy(ctx->stream);
+  if (r.stream) cudaStreamDestroy(r.stream);
   delete ctx;
   return SMAUG_OK;
 }
 
 int smaug_set_metric(smaug_ctx *ctx, const double *delx, size_t count) {
   if (!ctx || !delx) return SMAUG_ERR_ARG;
-  const int D = ctx->D;
-  const long long N = ctx->geo.N;
+  Run &r = ctx->run;
+  if (!r.sc) return fail(ctx, SMAUG_ERR_STATE, "context not created");
+  const int D = r.D;
+  const long long N = r.geo.N;
   if (count != (size_t)D * (size_t)N) return fail(ctx, SMAUG_ERR_ARG, "metric must hold ndim * N doubles");
   CK(cudaSetDevice(ctx->device));
-  // 1-D metric per dim from an inner line; the stencils use delx at inner
-  // cells only, where the reference's metric depends on that coordinate alone.
-  std::vector<double> d1(ctx->geo.n[0] + ctx->geo.n[1] + ctx->geo.n[2]);
+  // The stencils use delx at inner cells only, where the reference's metric
+  // depends on that coordinate alone: keep one line per dim.
+  std::vector<double> d1(r.geo.n[0] + r.geo.n[1] + r.geo.n[2]);
+  double minsq[3];
+  if (const char *m = metric_host(r, delx, d1.data(), minsq)) return fail(ctx, SMAUG_ERR_ARG, m);
+  CK(cudaMemcpyAsync(ctx->dx1, d1.data(), sizeof(double) * d1.size(), cudaMemcpyHostToDevice, r.stream));
   size_t off = 0;
   for (int d = 0; d < D; ++d) {
-    const double *m = delx + (size_t)d * N;
-    const int n = ctx->geo.n[d];
-    for (int x = 0; x < n; ++x) {
-      int c[3] = {2, 2, D == 3 ? 2 : 0};
-      c[d] = x;
-      d1[off + x] = m[c[0] + c[1] * ctx->geo.st[1] + c[2] * ctx->geo.st[2]];
-    }
-    // verify on all inner cells
-    for (long long j = 0; j < N; ++j) {
-      long long r = j;
-      int c[3];
-      c[0] = (int)(r % ctx->geo.n[0]);
-      r /= ctx->geo.n[0];
-      c[1] = (int)(r % ctx->geo.n[1]);
-      c[2] = (int)(r / ctx->geo.n[1]);
-      bool inner = true;
-      for (int e = 0; e < D; ++e)
-        if (c[e] < 2 || c[e] > ctx->geo.n[e] - 3) inner = false;
-      if (inner && m[j] != d1[off + c[d]])
-        return fail(ctx, SMAUG_ERR_ARG, "metric is not a tensor-product grid on the inner cells");
-      if (!(m[j] > 0.0)) return fail(ctx, SMAUG_ERR_ARG, "metric entries must be positive");
-    }
-    off += n;
-  }
-  CK(cudaMemcpyAsync(ctx->dx1, d1.data(), sizeof(double) * d1.size(), cudaMemcpyHostToDevice, ctx->stream));
-  off = 0;
-  for (int d = 0; d < D; ++d) {
-    ctx->geo.dx1[d] = ctx->dx1 + off;
-    off += ctx->geo.n[d];
+    r.geo.dx1[d] = ctx->dx1 + off;
+    off += r.geo.n[d];
   }
   CK(cudaMemcpyAsync(ctx->dxlast, delx + (size_t)(D - 1) * N, sizeof(double) * N, cudaMemcpyHostToDevice,
-                     ctx->stream));
-  ctx->geo.dxlast = ctx->dxlast;
-  // min over the first K cells of delx^2 (zeropadmaxdtvisc's cells)
-  for (int d = 0; d < D; ++d) {
-    double mn = INFINITY;
-    const double *m = delx + (size_t)d * N;
-    for (long long j = 0; j < ctx->geo.K && j < N; ++j) {
-      double v = (m[j]) * (m[j]);
-      if (v < mn) mn = v;
-    }
-    ctx->phys.minsq[d] = mn;
-  }
-  CK(cudaStreamSynchronize(ctx->stream));
+                     r.stream));
+  r.geo.dxlast = ctx->dxlast;
+  CK(cudaMemcpyAsync(r.sc->minsq, minsq, sizeof(minsq), cudaMemcpyHostToDevice, r.stream));
+  CK(cudaStreamSynchronize(r.stream));
   ctx->have_metric = true;
   return SMAUG_OK;
 }
 
 static int load_state(smaug_ctx *ctx, const double *w, size_t count, cudaMemcpyKind kind) {
   if (!ctx || !w) return SMAUG_ERR_ARG;
+  Run &r = ctx->run;
   if (!ctx->have_metric) return fail(ctx, SMAUG_ERR_STATE, "smaug_set_metric must come first");
-  const long long N = ctx->geo.N;
-  if (count != (size_t)ctx->NVAR * (size_t)N) return fail(ctx, SMAUG_ERR_ARG, "state must hold NVAR * N doubles");
+  const long long N = r.geo.N;
+  if (count != (size_t)r.NVAR * (size_t)N) return fail(ctx, SMAUG_ERR_ARG, "state must hold NVAR * N doubles");
   CK(cudaSetDevice(ctx->device));
-  ctx->cur = 0;
-  CK(cudaMemcpyAsync(ctx->W[0], w, sizeof(double) * N * ctx->NW, kind, ctx->stream));
-  CK(cudaMemcpyAsync(ctx->bg, w + (size_t)N * ctx->NW, sizeof(double) * N * ctx->NB, kind, ctx->stream));
+  CK(cudaMemcpyAsync(r.W[0], w, sizeof(double) * N * r.NW, kind, r.stream));
+  CK(cudaMemcpyAsync(r.bg, w + (size_t)N * r.NW, sizeof(double) * N * r.NB, kind, r.stream));
   // host-side scan of the backgrounds: are the energy background terms live?
   if (kind == cudaMemcpyHostToDevice) {
     int has = 0;
-    const double *b = w + (size_t)N * ctx->NW;
+    const double *b = w + (size_t)N * r.NW;
     for (long long j = 0; j < N && !has; ++j) {
       if (b[j] != 0.0) has = 1;  // eb
-      for (int k = 0; k < ctx->D; ++k)
+      for (int k = 0; k < r.D; ++k)
         if (b[(size_t)(2 + k) * N + j] != 0.0) has = 1;
     }
-    ctx->phys.has_bgb = has;
+    r.phys.has_bgb = has;
   } else {
-    ctx->phys.has_bgb = 1;
+    r.phys.has_bgb = 1;
   }
-  ghost_fill_kernel<<<148 * 8, 256, 0, ctx->stream>>>(ctx->W[0], ctx->NW, ctx->geo, ctx->D);
-  DevScalars init{};
-  init.dt = ctx->prm.dt_mode == 1 ? 1.0e-8 : ctx->prm.dt0;
-  if (ctx->prm.dt_mode == 1 && ctx->prm.dt0 > 0) init.dt = ctx->prm.dt0;
-  CK(cudaMemcpyAsync(ctx->sc, &init, sizeof(DevScalars), cudaMemcpyHostToDevice, ctx->stream));
-  if (ctx->prm.exact)
-    smaug_exact::launch_reduce(ctx->D, ctx->W[0], ctx->bg, ctx->geo, ctx->phys, &ctx->sc->red[0], ctx->stream);
-  else
-    smaug_fast::launch_reduce(ctx->D, ctx->W[0], ctx->bg, ctx->geo, ctx->phys, &ctx->sc->red[0], ctx->stream);
-  ctx->launches += 2;
-  CK(cudaGetLastError());
-  CK(cudaStreamSynchronize(ctx->stream));
+  CK(run_load(r));
+  CK(cudaStreamSynchronize(r.stream));
   ctx->have_state = true;
   ctx->steps = 0;
   return SMAUG_OK;
@@ -373,13 +449,14 @@ int smaug_set_state_device(smaug_ctx *ctx, const double *w, size_t count) {
 
 static int store_state(smaug_ctx *ctx, double *w, size_t count, cudaMemcpyKind kind, bool sync) {
   if (!ctx || !w) return SMAUG_ERR_ARG;
+  Run &r = ctx->run;
   if (!ctx->have_state) return fail(ctx, SMAUG_ERR_STATE, "no state loaded");
-  const long long N = ctx->geo.N;
-  if (count != (size_t)ctx->NVAR * (size_t)N) return fail(ctx, SMAUG_ERR_ARG, "state must hold NVAR * N doubles");
+  const long long N = r.geo.N;
+  if (count != (size_t)r.NVAR * (size_t)N) return fail(ctx, SMAUG_ERR_ARG, "state must hold NVAR * N doubles");
   CK(cudaSetDevice(ctx->device));
-  CK(cudaMemcpyAsync(w, ctx->W[ctx->cur], sizeof(double) * N * ctx->NW, kind, ctx->stream));
-  CK(cudaMemcpyAsync(w + (size_t)N * ctx->NW, ctx->bg, sizeof(double) * N * ctx->NB, kind, ctx->stream));
-  if (sync) CK(cudaStreamSynchronize(ctx->stream));
+  CK(cudaMemcpyAsync(w, r.W[r.cur], sizeof(double) * N * r.NW, kind, r.stream));
+  CK(cudaMemcpyAsync(w + (size_t)N * r.NW, r.bg, sizeof(double) * N * r.NB, kind, r.stream));
+  if (sync) CK(cudaStreamSynchronize(r.stream));
   return SMAUG_OK;
 }
 
@@ -394,47 +471,19 @@ int smaug_step(smaug_ctx *ctx, int nsteps) {
   if (!ctx || nsteps < 0) return SMAUG_ERR_ARG;
   if (!ctx->have_state) return fail(ctx, SMAUG_ERR_STATE, "no state loaded");
   CK(cudaSetDevice(ctx->device));
-  for (int it = 0; it < nsteps; ++it) {
-    dt_kernel<<<1, 1, 0, ctx->stream>>>(ctx->sc, ctx->phys, ctx->D);
-    ctx->launches++;
-    StageArgs a{};
-    a.bg = ctx->bg;
-    a.sc = ctx->sc;
-    if (!ctx->prm.rk4) {
-      double *w = ctx->W[ctx->cur], *o = ctx->W[1 - ctx->cur];
-      a.in = w; a.base = w; a.out = o; a.acc = nullptr; a.kind = 0;
-      a.red_in = 0; a.red_out = 1; a.hdiv = 1.0;
-      launch_stage(ctx, a);
-      finish_kernel<<<1, 1, 0, ctx->stream>>>(ctx->sc, 1);
-      ctx->cur = 1 - ctx->cur;
-    } else {
-      // SAC fourstep (vac.t:447-462): W1 = W + dt/2 L(W); W2 = W + dt/2 L(W1);
-      // W3 = W + dt L(W2) and W1 <- (W1 + 2 W2 + W3 - 4 W)/3; W <- (W + dt/6 L(W3)) + W1
-      double *W = ctx->W[0], *W1 = ctx->W[1], *W2 = ctx->W[2], *W3 = ctx->W[3];
-      a.base = W;
-      a.in = W;  a.out = W1; a.acc = nullptr; a.kind = 0; a.red_in = 0; a.red_out = 1; a.hdiv = 2.0;
-      launch_stage(ctx, a);
-      a.in = W1; a.out = W2; a.red_in = 1; a.red_out = 2; a.hdiv = 2.0;
-      launch_stage(ctx, a);
-      a.in = W2; a.out = W3; a.acc = W1; a.kind = 3; a.red_in = 2; a.red_out = 3; a.hdiv = 1.0;
-      launch_stage(ctx, a);
-      a.in = W3; a.out = W;  a.acc = W1; a.kind = 4; a.red_in = 3; a.red_out = 4; a.hdiv = 6.0;
-      launch_stage(ctx, a);
-      finish_kernel<<<1, 1, 0, ctx->stream>>>(ctx->sc, 4);
-    }
-    ctx->launches++;
-    CK(cudaGetLastError());
-    ctx->steps++;
-  }
+  Run &r = ctx->run;
+  r.ev_used = ctx->profile ? &ctx->ev_used : nullptr;
+  CK(run_steps(r, nsteps));
+  ctx->steps += nsteps;
   return SMAUG_OK;
 }
 
 int smaug_sync(smaug_ctx *ctx) {
   if (!ctx) return SMAUG_ERR_ARG;
   CK(cudaSetDevice(ctx->device));
-  CK(cudaStreamSynchronize(ctx->stream));
+  CK(cudaStreamSynchronize(ctx->run.stream));
   int status = 0;
-  CK(cudaMemcpy(&status, &ctx->sc->status, sizeof(int), cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(&status, &ctx->run.sc->status, sizeof(int), cudaMemcpyDeviceToHost));
   if (status != 0) return fail(ctx, status, "non-finite dt or wave speed on the device");
   return SMAUG_OK;
 }
@@ -443,13 +492,13 @@ int smaug_get_scalars(smaug_ctx *ctx, double out[8]) {
   if (!ctx || !out) return SMAUG_ERR_ARG;
   CK(cudaSetDevice(ctx->device));
   DevScalars s;
-  CK(cudaStreamSynchronize(ctx->stream));
-  CK(cudaMemcpy(&s, ctx->sc, sizeof(DevScalars), cudaMemcpyDeviceToHost));
+  CK(cudaStreamSynchronize(ctx->run.stream));
+  CK(cudaMemcpy(&s, ctx->run.sc, sizeof(DevScalars), cudaMemcpyDeviceToHost));
   out[0] = s.dt;
   out[1] = s.maxcourant;
   out[2] = s.maxviscoef;
   out[3] = s.dtdiffvisc;
-  for (int d = 0; d < 3; ++d) out[4 + d] = d < ctx->D ? red_get(s.red[0], d) : 0.0;
+  for (int d = 0; d < 3; ++d) out[4 + d] = d < ctx->run.D ? red_get(s.red[0], d) : 0.0;
   out[7] = (double)ctx->steps;
   return SMAUG_OK;
 }
@@ -464,7 +513,7 @@ int smaug_profile_stages(smaug_ctx *ctx, int enable) {
 int smaug_stage_times(smaug_ctx *ctx, double *ms_total, long long *count) {
   if (!ctx || !ms_total || !count) return SMAUG_ERR_ARG;
   CK(cudaSetDevice(ctx->device));
-  CK(cudaStreamSynchronize(ctx->stream));
+  CK(cudaStreamSynchronize(ctx->run.stream));
   double t = 0.0;
   for (size_t i = 0; i + 1 < ctx->ev_used; i += 2) {
     float ms = 0.f;
@@ -477,8 +526,8 @@ int smaug_stage_times(smaug_ctx *ctx, double *ms_total, long long *count) {
   return SMAUG_OK;
 }
 
-void *smaug_stream(smaug_ctx *ctx) { return ctx ? (void *)ctx->stream : nullptr; }
-long long smaug_launch_count(smaug_ctx *ctx) { return ctx ? ctx->launches : 0; }
+void *smaug_stream(smaug_ctx *ctx) { return ctx ? (void *)ctx->run.stream : nullptr; }
+long long smaug_launch_count(smaug_ctx *ctx) { return ctx ? ctx->run.launches : 0; }
 const char *smaug_last_error(smaug_ctx *ctx) { return ctx ? ctx->err.c_str() : "null context"; }
 
 }  // extern "C"

@@ -33,9 +33,9 @@ struct DevScalars {
   double dtdiffvisc;
   double maxviscoef;  // running maximum over all steps
   double maxcourant;
+  double minsq[3];    // min over the first K cells of delx_d^2 (viscous dt), set with the metric
   int step;
   int status;
-  int pad[2];
   Reduce red[5];  // [0] state at step start, [1..3] RK stage outputs, [4] state at step end
 };
 
@@ -54,7 +54,6 @@ struct Phys {
   double courant;
   double chyp[13];
   double g[3];
-  double minsq[3];            // min over the first K cells of delx_d^2 (viscous dt)
   int hyperdif;
   int has_bgb;                // any background B or eb != 0 (energy background terms)
   int has_grav;
