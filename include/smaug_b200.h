@@ -114,6 +114,39 @@ int smaug_get_scalars(smaug_ctx *ctx, double out[8]);
 int smaug_profile_stages(smaug_ctx *ctx, int enable);
 int smaug_stage_times(smaug_ctx *ctx, double *ms_total, long long *count);
 
+/*
+ * smaug_step_noalloc -- no counterpart in the reference.
+ *
+ * One call advances a state by nsteps steps without allocating any device
+ * memory, for callers that cannot call cudaMalloc: a framework whose caching
+ * allocator owns the GPU's memory (a raw cudaMalloc would then fail or
+ * fragment it), code that must not allocate once its set-up is done (a
+ * real-time or serving loop with a fixed memory budget), or a host that only
+ * holds device pointers handed to it by someone else.
+ *
+ * The caller passes everything by device pointer: the metric (ndim * N
+ * doubles, as for smaug_set_metric), the input state and the output state
+ * (NVAR * N doubles each, layout above; w_out may equal w_in).  The
+ * Runge-Kutta stage buffers and the device-side scalars live in a file-scope
+ * device array of SMAUG_NOALLOC_SCRATCH_BYTES that every GPU which loads the
+ * library holds until the process exits.  Grids whose scratch would not fit
+ * (3 * (2 + 2*ndim) * N doubles plus the metric lines and the scalars) are
+ * rejected with SMAUG_ERR_ARG and a message in err.
+ *
+ * Each call starts afresh from w_in (dt from dt0 / the reference's dt rule,
+ * counters cleared); the scratch keeps the previous call's contents, so calls
+ * whose work overlaps on the GPU (different streams, other threads) race on
+ * it and must be serialised by the caller.  The first call on a device looks
+ * up the scratch address (cudaGetSymbolAddress); make that first call before
+ * any stream capture.  The call waits for its stream before returning;
+ * scalars_out (8 doubles, as smaug_get_scalars, may be NULL) and err (may be
+ * NULL) are host buffers.
+ */
+#define SMAUG_NOALLOC_SCRATCH_BYTES (32u << 20)
+int smaug_step_noalloc(const smaug_params *prm, const double *delx_dev, const double *w_in_dev,
+                       double *w_out_dev, int nsteps, void *stream, double *scalars_out, char *err,
+                       size_t errlen);
+
 /* The CUDA stream (cudaStream_t) all work of ctx is ordered on. */
 void *smaug_stream(smaug_ctx *ctx);
 

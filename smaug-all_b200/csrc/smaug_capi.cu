@@ -272,6 +272,52 @@ cudaError_t run_steps(Run &r, int nsteps) {
   return cudaSuccess;
 }
 
+// Device-side metric set-up for smaug_step_noalloc, whose metric already sits
+// in device memory: the 1-D metric of each dim along an inner line, a
+// tensor-product check on the inner cells (status flag), and the minimum of
+// delx_d^2 over the first K cells as an order-preserving atomic minimum on the
+// bit patterns of positive doubles (minsq must start at +inf).
+__global__ void metric_kernel(const double *delx, Geo g, int D, double *dx1, DevScalars *sc) {
+  const long long tid = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  const long long nthr = (long long)gridDim.x * blockDim.x;
+  long long off = 0;
+  for (int d = 0; d < D; ++d) {
+    for (long long x = tid; x < g.n[d]; x += nthr) {
+      int c[3] = {2, 2, D == 3 ? 2 : 0};
+      c[d] = (int)x;
+      dx1[off + x] = delx[(long long)d * g.N + c[0] + c[1] * g.st[1] + c[2] * g.st[2]];
+    }
+    off += g.n[d];
+  }
+  for (long long j = tid; j < g.N; j += nthr) {
+    long long q = j;
+    int c[3];
+    c[0] = (int)(q % g.n[0]);
+    q /= g.n[0];
+    c[1] = (int)(q % g.n[1]);
+    c[2] = (int)(q / g.n[1]);
+    bool inner = true;
+    for (int e = 0; e < D; ++e)
+      if (c[e] < 2 || c[e] > g.n[e] - 3) inner = false;
+    for (int d = 0; d < D; ++d) {
+      const double v = delx[(long long)d * g.N + j];
+      if (!(v > 0.0)) atomicExch(&sc->status, (int)SMAUG_ERR_ARG);
+      if (inner) {
+        int cl[3] = {2, 2, D == 3 ? 2 : 0};
+        cl[d] = c[d];
+        if (v != delx[(long long)d * g.N + cl[0] + cl[1] * g.st[1] + cl[2] * g.st[2]])
+          atomicExch(&sc->status, (int)SMAUG_ERR_ARG);
+      }
+      if (j < g.K) atomicMin((unsigned long long *)&sc->minsq[d], (unsigned long long)__double_as_longlong(v * v));
+    }
+  }
+}
+
+__global__ void minsq_init_kernel(DevScalars *sc) {
+  if (threadIdx.x == 0 && blockIdx.x == 0)
+    for (int d = 0; d < 3; ++d) sc->minsq[d] = INFINITY;
+}
+
 // 1-D metric lines, tensor-product check and min delx^2 over the first K
 // cells, from a host metric (ndim * N doubles).  Returns an error or nullptr.
 const char *metric_host(const Run &r, const double *delx, double *d1, double minsq[3]) {
@@ -523,6 +569,132 @@ int smaug_stage_times(smaug_ctx *ctx, double *ms_total, long long *count) {
   *ms_total = t;
   *count = (long long)(ctx->ev_used / 2);
   ctx->ev_used = 0;
+  return SMAUG_OK;
+}
+
+// ---------------------------------------------------------------------------
+// smaug_step_noalloc: the RK step for callers that cannot allocate device
+// memory.  Its scratch (the three Runge-Kutta stage buffers, the device-side
+// scalars and the 1-D metric lines) lives in this file-scope device array,
+// which every GPU that loads the library holds until the process exits.
+// Host code must not use g_noalloc_scratch as an address: it is a host-side
+// stand-in for the symbol; the device address comes from
+// cudaGetSymbolAddress, once per device, in noalloc_scratch().
+// ---------------------------------------------------------------------------
+static __device__ __align__(256) unsigned char g_noalloc_scratch[SMAUG_NOALLOC_SCRATCH_BYTES];
+
+namespace {
+constexpr int kMaxDevices = 64;
+void *g_scratch_addr[kMaxDevices] = {nullptr};
+
+void set_err(char *err, size_t errlen, const char *msg) {
+  if (err && errlen) {
+    std::strncpy(err, msg, errlen - 1);
+    err[errlen - 1] = '\0';
+  }
+}
+
+// Device address of the scratch array on the current device (looked up on
+// the first call per device).
+cudaError_t noalloc_scratch(void **out) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  if (dev < 0 || dev >= kMaxDevices) return cudaErrorInvalidDevice;
+  if (!g_scratch_addr[dev]) {
+    void *p = nullptr;
+    e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess) return e;
+    g_scratch_addr[dev] = p;
+  }
+  *out = g_scratch_addr[dev];
+  return cudaSuccess;
+}
+}  // namespace
+
+int smaug_step_noalloc(const smaug_params *prm, const double *delx_dev, const double *w_in_dev, double *w_out_dev,
+                       int nsteps, void *stream, double *scalars_out, char *err, size_t errlen) {
+  if (!prm || !delx_dev || !w_in_dev || !w_out_dev || nsteps < 0) {
+    set_err(err, errlen, "null argument or negative step count");
+    return SMAUG_ERR_ARG;
+  }
+  Run r;
+  if (const char *m = plan(prm, r)) {
+    set_err(err, errlen, m);
+    return SMAUG_ERR_ARG;
+  }
+  const long long N = r.geo.N;
+  const size_t head = (sizeof(DevScalars) + 255) / 256 * 256;
+  const size_t lines = ((size_t)(r.geo.n[0] + r.geo.n[1] + r.geo.n[2]) * sizeof(double) + 255) / 256 * 256;
+  const size_t field = ((size_t)r.NW * (size_t)N * sizeof(double) + 255) / 256 * 256;
+  const size_t need = head + lines + 3 * field;
+  if (need > (size_t)SMAUG_NOALLOC_SCRATCH_BYTES) {
+    char msg[160];
+    std::snprintf(msg, sizeof(msg), "grid needs %zu bytes of scratch, above the %u-byte maximum of smaug_step_noalloc",
+                  need, (unsigned)SMAUG_NOALLOC_SCRATCH_BYTES);
+    set_err(err, errlen, msg);
+    return SMAUG_ERR_ARG;
+  }
+  void *base = nullptr;
+  cudaError_t e = noalloc_scratch(&base);
+  if (e != cudaSuccess) {
+    set_err(err, errlen, cudaGetErrorString(e));
+    return SMAUG_ERR_CUDA;
+  }
+  unsigned char *s = (unsigned char *)base;
+  r.stream = (cudaStream_t)stream;
+  r.sc = (DevScalars *)s;
+  double *dx1 = (double *)(s + head);
+  r.W[0] = w_out_dev;
+  r.bg = w_out_dev + (size_t)r.NW * N;
+  for (int k = 0; k < 3; ++k) r.W[1 + k] = (double *)(s + head + lines + k * field);
+  size_t off = 0;
+  for (int d = 0; d < r.D; ++d) {
+    r.geo.dx1[d] = dx1 + off;
+    off += r.geo.n[d];
+  }
+  r.geo.dxlast = delx_dev + (size_t)(r.D - 1) * N;
+  r.phys.has_bgb = 1;
+#define NA(call)                                \
+  do {                                          \
+    cudaError_t e_ = (call);                    \
+    if (e_ != cudaSuccess) {                    \
+      set_err(err, errlen, cudaGetErrorString(e_)); \
+      return SMAUG_ERR_CUDA;                    \
+    }                                           \
+  } while (0)
+  if (w_out_dev != w_in_dev)
+    NA(cudaMemcpyAsync(w_out_dev, w_in_dev, sizeof(double) * (size_t)r.NVAR * N, cudaMemcpyDeviceToDevice, r.stream));
+  // every call starts from cleared scalars: the array keeps the last call's data
+  NA(cudaMemsetAsync(r.sc, 0, sizeof(DevScalars), r.stream));
+  NA(run_load(r));  // ghost fill of w_out, scalars reset, initial maxima
+  minsq_init_kernel<<<1, 1, 0, r.stream>>>(r.sc);
+  metric_kernel<<<148 * 4, 256, 0, r.stream>>>(delx_dev, r.geo, r.D, dx1, r.sc);
+  NA(cudaGetLastError());
+  NA(run_steps(r, nsteps));
+  if (r.cur != 0)  // single-step mode with an odd step count: result in W[1]
+    NA(cudaMemcpyAsync(w_out_dev, r.W[1], sizeof(double) * (size_t)r.NW * N, cudaMemcpyDeviceToDevice, r.stream));
+  DevScalars hs;
+  NA(cudaMemcpyAsync(&hs, r.sc, sizeof(DevScalars), cudaMemcpyDeviceToHost, r.stream));
+  NA(cudaStreamSynchronize(r.stream));
+#undef NA
+  if (scalars_out) {
+    scalars_out[0] = hs.dt;
+    scalars_out[1] = hs.maxcourant;
+    scalars_out[2] = hs.maxviscoef;
+    scalars_out[3] = hs.dtdiffvisc;
+    for (int d = 0; d < 3; ++d) scalars_out[4 + d] = d < r.D ? red_get(hs.red[0], d) : 0.0;
+    scalars_out[7] = (double)nsteps;
+  }
+  if (hs.status == SMAUG_ERR_ARG) {
+    set_err(err, errlen, "metric is not positive or not a tensor-product grid on the inner cells");
+    return SMAUG_ERR_ARG;
+  }
+  if (hs.status != 0) {
+    set_err(err, errlen, "non-finite dt or wave speed on the device");
+    return hs.status;
+  }
+  set_err(err, errlen, "");
   return SMAUG_OK;
 }
 
