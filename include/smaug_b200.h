@@ -54,6 +54,17 @@ enum {
 /* Boundary types per direction (iotypes.h:145 boundtype codes). */
 enum { SMAUG_BC_PERIODIC = 0, SMAUG_BC_CONTCD4 = 4 };
 
+/*
+ * Arithmetic of the step.  The reference computes everything in FP64 (real =
+ * double, iotypes.h).  SMAUG_PREC_MIXED (no counterpart in the reference)
+ * keeps the stage states and the stencil arithmetic in FP32 and FP64 where
+ * accuracy needs it: background fields, total pressure and internal energy
+ * (recovered by cancellation), the RK base state (an FP32 value plus an FP32
+ * compensation), the RK combination and the dt reductions.  Needs rk4 = 1 and
+ * exact = 0; host buffers stay FP64.
+ */
+enum { SMAUG_PREC_FP64 = 0, SMAUG_PREC_MIXED = 1 };
+
 typedef struct smaug_ctx smaug_ctx;
 
 typedef struct {
@@ -69,6 +80,7 @@ typedef struct {
   int dt_mode;      /* 1: dt from the reference's moddton rule; 0: fixed dt = dt0 */
   double dt0;       /* initial dt (1e-8 when dt_mode = 1, iosmaug.cpp:327-330) */
   int exact;        /* 1: kernels built without FMA contraction (bit-reproducible) */
+  int precision;    /* SMAUG_PREC_FP64 (default, 0) or SMAUG_PREC_MIXED */
 } smaug_params;
 
 /* Number of fields for ndim (10 or 13). */
@@ -140,7 +152,7 @@ int smaug_stage_times(smaug_ctx *ctx, double *ms_total, long long *count);
  * up the scratch address (cudaGetSymbolAddress); make that first call before
  * any stream capture.  The call waits for its stream before returning;
  * scalars_out (8 doubles, as smaug_get_scalars, may be NULL) and err (may be
- * NULL) are host buffers.
+ * NULL) are host buffers.  FP64 only: precision must be SMAUG_PREC_FP64.
  */
 #define SMAUG_NOALLOC_SCRATCH_BYTES (32u << 20)
 int smaug_step_noalloc(const smaug_params *prm, const double *delx_dev, const double *w_in_dev,

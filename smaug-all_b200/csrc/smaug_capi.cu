@@ -23,12 +23,14 @@
 #include "smaug_device.cuh"
 
 namespace smaug_exact {
-void launch_stage(int D, const smaug::StageArgs &a, const smaug::Geo &g, const smaug::Phys &p, cudaStream_t st);
+void launch_stage(int D, bool mixed, const smaug::StageArgs &a, const smaug::Geo &g, const smaug::Phys &p,
+                  cudaStream_t st);
 void launch_reduce(int D, const double *w, const double *bg, const smaug::Geo &g, const smaug::Phys &p,
                    smaug::Reduce *r, cudaStream_t st);
 }  // namespace smaug_exact
 namespace smaug_fast {
-void launch_stage(int D, const smaug::StageArgs &a, const smaug::Geo &g, const smaug::Phys &p, cudaStream_t st);
+void launch_stage(int D, bool mixed, const smaug::StageArgs &a, const smaug::Geo &g, const smaug::Phys &p,
+                  cudaStream_t st);
 void launch_reduce(int D, const double *w, const double *bg, const smaug::Geo &g, const smaug::Phys &p,
                    smaug::Reduce *r, cudaStream_t st);
 }  // namespace smaug_fast
@@ -43,10 +45,13 @@ struct Run {
   int D = 0, NW = 0, NB = 0, NVAR = 0;
   Geo geo{};
   Phys phys{};
-  bool rk4 = true, exact = false;
+  bool rk4 = true, exact = false, mixed = false;
   double dt0 = 0.0;
   cudaStream_t stream = nullptr;
   double *W[4] = {nullptr, nullptr, nullptr, nullptr};  // state, then RK stages (or ping-pong)
+  // mixed precision: FP32 base value, its FP32 compensation, two FP32 stage
+  // states and the FP32 RK increment sum (W[0] then only stages loads/stores)
+  float *F[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
   double *bg = nullptr;
   DevScalars *sc = nullptr;
   int cur = 0;
@@ -107,6 +112,10 @@ const char *plan(const smaug_params *prm, Run &r) {
   r.rk4 = prm->rk4 != 0;
   r.exact = prm->exact != 0;
   r.dt0 = prm->dt0;
+  if (prm->precision != SMAUG_PREC_FP64 && prm->precision != SMAUG_PREC_MIXED)
+    return "precision must be SMAUG_PREC_FP64 (0) or SMAUG_PREC_MIXED (1)";
+  r.mixed = prm->precision == SMAUG_PREC_MIXED;
+  if (r.mixed && (!r.rk4 || r.exact)) return "mixed precision needs rk4 = 1 and exact = 0";
   return nullptr;
 }
 
@@ -213,15 +222,33 @@ void launch_stage(Run &r, const StageArgs &a) {
     }
   }
   if (r.exact)
-    smaug_exact::launch_stage(r.D, a, r.geo, r.phys, r.stream);
+    smaug_exact::launch_stage(r.D, false, a, r.geo, r.phys, r.stream);
   else
-    smaug_fast::launch_stage(r.D, a, r.geo, r.phys, r.stream);
+    smaug_fast::launch_stage(r.D, r.mixed, a, r.geo, r.phys, r.stream);
   if (e1) cudaEventRecord(e1, r.stream);
   r.launches++;
 }
 
+// FP64 state -> FP32 value + FP32 compensation (w = hi + lo to ~48 bits).
+__global__ void split_kernel(const double *__restrict__ w, float *__restrict__ hi, float *__restrict__ lo, long long n) {
+  for (long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x; j < n; j += (long long)gridDim.x * blockDim.x) {
+    const double v = w[j];
+    const float h = (float)v;
+    hi[j] = h;
+    lo[j] = (float)(v - (double)h);
+  }
+}
+
+// FP32 value + compensation -> FP64 state.
+__global__ void combine_kernel(const float *__restrict__ hi, const float *__restrict__ lo, double *__restrict__ w,
+                               long long n) {
+  for (long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x; j < n; j += (long long)gridDim.x * blockDim.x)
+    w[j] = (double)hi[j] + (double)lo[j];
+}
+
 // A state is in r.W[0] (evolved) and r.bg: fill ghosts, reset scalars,
-// reduce the initial maxima.  Asynchronous.
+// reduce the initial maxima (and, mixed, split it into value +
+// compensation).  Asynchronous.
 cudaError_t run_load(Run &r) {
   r.cur = 0;
   ghost_fill_kernel<<<148 * 8, 256, 0, r.stream>>>(r.W[0], r.NW, r.geo, r.D);
@@ -232,6 +259,18 @@ cudaError_t run_load(Run &r) {
   else
     smaug_fast::launch_reduce(r.D, r.W[0], r.bg, r.geo, r.phys, &r.sc->red[0], r.stream);
   r.launches += 3;
+  if (r.mixed) {
+    split_kernel<<<148 * 8, 256, 0, r.stream>>>(r.W[0], r.F[0], r.F[1], (long long)r.NW * r.geo.N);
+    r.launches++;
+  }
+  return cudaGetLastError();
+}
+
+// Mixed precision: bring the FP64 copy W[0] up to date with w32 + c32.
+cudaError_t run_combine(Run &r) {
+  if (!r.mixed) return cudaSuccess;
+  combine_kernel<<<148 * 8, 256, 0, r.stream>>>(r.F[0], r.F[1], r.W[0], (long long)r.NW * r.geo.N);
+  r.launches++;
   return cudaGetLastError();
 }
 
@@ -243,7 +282,22 @@ cudaError_t run_steps(Run &r, int nsteps) {
     StageArgs a{};
     a.bg = r.bg;
     a.sc = r.sc;
-    if (!r.rk4) {
+    if (r.mixed) {
+      // the same fourstep with FP32 stage states: S1 = W + dt/2 L(W),
+      // S2 = W + dt/2 L(S1), S3 = W + dt L(S2), A = (S1 + 2 S2 + S3 - 4 W)/3
+      // accumulated stage by stage, W <- W + dt/6 L(S3) + A
+      float *w32 = r.F[0], *c32 = r.F[1], *sa = r.F[2], *sb = r.F[3], *acc = r.F[4];
+      a.w32 = w32; a.c32 = c32; a.acc32 = acc;
+      a.in32 = w32; a.out32 = sa; a.kind = 1; a.red_in = 0; a.red_out = 1; a.hdiv = 2.0;
+      launch_stage(r, a);
+      a.in32 = sa;  a.out32 = sb; a.kind = 2; a.red_in = 1; a.red_out = 2; a.hdiv = 2.0;
+      launch_stage(r, a);
+      a.in32 = sb;  a.out32 = sa; a.kind = 3; a.red_in = 2; a.red_out = 3; a.hdiv = 1.0;
+      launch_stage(r, a);
+      a.in32 = sa;  a.out32 = nullptr; a.kind = 4; a.red_in = 3; a.red_out = 4; a.hdiv = 6.0;
+      launch_stage(r, a);
+      finish_kernel<<<1, 1, 0, r.stream>>>(r.sc, 4);
+    } else if (!r.rk4) {
       double *w = r.W[r.cur], *o = r.W[1 - r.cur];
       a.in = w; a.base = w; a.out = o; a.acc = nullptr; a.kind = 0;
       a.red_in = 0; a.red_out = 1; a.hdiv = 1.0;
@@ -403,7 +457,9 @@ int smaug_create(const smaug_params *prm, int device, smaug_ctx **out) {
   CK(cudaSetDevice(device));
   CK(cudaStreamCreateWithFlags(&r.stream, cudaStreamNonBlocking));
   const size_t fsz = sizeof(double) * (size_t)r.geo.N;
-  for (int b = 0; b < 4; ++b) CK(cudaMalloc(&r.W[b], fsz * r.NW));
+  for (int b = 0; b < (r.mixed ? 1 : 4); ++b) CK(cudaMalloc(&r.W[b], fsz * r.NW));
+  if (r.mixed)
+    for (auto &f : r.F) CK(cudaMalloc(&f, sizeof(float) * (size_t)r.geo.N * r.NW));
   CK(cudaMalloc(&r.bg, fsz * r.NB));
   CK(cudaMalloc(&ctx->dx1, sizeof(double) * (r.geo.n[0] + r.geo.n[1] + r.geo.n[2])));
   CK(cudaMalloc(&ctx->dxlast, fsz));
@@ -419,6 +475,7 @@ int smaug_destroy(smaug_ctx *ctx) {
   cudaSetDevice(ctx->device);
   if (r.stream) cudaStreamSynchronize(r.stream);
   for (auto &b : r.W) cudaFree(b);
+  for (auto &f : r.F) cudaFree(f);
   cudaFree(r.bg);
   cudaFree(ctx->dx1);
   cudaFree(ctx->dxlast);
@@ -500,6 +557,7 @@ static int store_state(smaug_ctx *ctx, double *w, size_t count, cudaMemcpyKind k
   const long long N = r.geo.N;
   if (count != (size_t)r.NVAR * (size_t)N) return fail(ctx, SMAUG_ERR_ARG, "state must hold NVAR * N doubles");
   CK(cudaSetDevice(ctx->device));
+  CK(run_combine(r));
   CK(cudaMemcpyAsync(w, r.W[r.cur], sizeof(double) * N * r.NW, kind, r.stream));
   CK(cudaMemcpyAsync(w + (size_t)N * r.NW, r.bg, sizeof(double) * N * r.NB, kind, r.stream));
   if (sync) CK(cudaStreamSynchronize(r.stream));
@@ -621,6 +679,10 @@ int smaug_step_noalloc(const smaug_params *prm, const double *delx_dev, const do
   Run r;
   if (const char *m = plan(prm, r)) {
     set_err(err, errlen, m);
+    return SMAUG_ERR_ARG;
+  }
+  if (r.mixed) {
+    set_err(err, errlen, "smaug_step_noalloc runs the FP64 path only (precision = 0)");
     return SMAUG_ERR_ARG;
   }
   const long long N = r.geo.N;

@@ -61,13 +61,18 @@ struct Phys {
 };
 
 struct StageArgs {
+  // FP64 path
   const double *in;    // NW evolved fields, stage input (read with halo)
-  const double *bg;    // NB background fields
+  const double *bg;    // NB background fields (FP64 in both paths)
   const double *base;  // NW evolved fields, RK base (read at the cell)
   double *out;         // NW evolved fields, stage output
   double *acc;         // RK accumulator (stage 3 writes (w1+2w2+w3-4w)/3, stage 4 adds it)
+  // mixed-precision path: FP32 stage states, the RK base as an FP32 value plus
+  // an FP32 compensation (w32 + c32 carries ~48 bits), FP32 RK increment sum
+  const float *in32;
+  float *out32, *acc32, *w32, *c32;
   DevScalars *sc;
-  int kind;            // 0 plain, 3 = RK stage 3, 4 = RK stage 4
+  int kind;            // FP64: 0 plain, 3 = RK stage 3, 4 = RK stage 4; mixed: RK stage 1..4
   int red_in, red_out; // reduction slots: cmax of `in`, maxima of `out`
   double hdiv;         // h = dt / hdiv (dt/2, dt/2, dt, dt/6 as the oracle divides)
 };

@@ -13,22 +13,32 @@
 //  * divisions become multiplications by per-cell reciprocals.
 // Results match the reference operator to rounding (the FMA-free restatement
 // in smaug_stage.cuh is the bit-exact one).
+//
+// The template parameter T is the type of the stage states and of the stencil
+// arithmetic: double (the FP64 path) or float (the mixed path).  The mixed
+// path keeps FP64 where accuracy needs it: the background fields, the total
+// pressure p_T and the internal energy (both recovered by cancellation), the
+// RK base state (an FP32 value plus an FP32 compensation), the RK combination
+// itself and the dt reductions.  With T = double every expression below is
+// the FP64 path's.
 #pragma once
 #include "smaug_device.cuh"
 
 namespace SMAUG_NS {
 using namespace smaug;
 
+// A tile of inner cells, one thread per cell (TZ = 1 in 2-D).
+template <int X, int Y, int Z>
+struct Tile {
+  static constexpr int TX = X, TY = Y, TZ = Z, NT = X * Y * Z;
+};
+// the single-instance kernels' tiles
 template <int D>
 struct TileShape;
 template <>
-struct TileShape<2> {
-  static constexpr int TX = 16, TY = 16, TZ = 1;
-};
+struct TileShape<2> : Tile<16, 16, 1> {};
 template <>
-struct TileShape<3> {
-  static constexpr int TX = 8, TY = 8, TZ = 4;
-};
+struct TileShape<3> : Tile<8, 8, 4> {};
 
 template <int D>
 struct TileBox {
@@ -51,6 +61,27 @@ __device__ __forceinline__ long long gidx(const Geo &g, const int *c) {
   return c[0] + (long long)c[1] * g.st[1] + (D == 3 ? (long long)c[2] * g.st[2] : 0);
 }
 
+__device__ __forceinline__ double vmax(double a, double b) { return fmax(a, b); }
+__device__ __forceinline__ float vmax(float a, float b) { return fmaxf(a, b); }
+__device__ __forceinline__ double vabs(double a) { return fabs(a); }
+__device__ __forceinline__ float vabs(float a) { return fabsf(a); }
+
+// State accessor: evolved fields of type T, background fields FP64.
+template <int D, typename T>
+struct CellT {
+  const T *__restrict__ in;
+  const double *__restrict__ bg;
+  long long N;
+  // field f at cell i in the stencil type
+  __device__ __forceinline__ T v(int f, long long i) const {
+    return f < Lay<D>::NW ? __ldg(in + (long long)f * N + i) : (T)__ldg(bg + (long long)(f - Lay<D>::NW) * N + i);
+  }
+  // field f at cell i in FP64
+  __device__ __forceinline__ double vd(int f, long long i) const {
+    return f < Lay<D>::NW ? (double)__ldg(in + (long long)f * N + i) : __ldg(bg + (long long)(f - Lay<D>::NW) * N + i);
+  }
+};
+
 template <int D>
 __device__ __forceinline__ bool in_grid(const Geo &g, const int *c) {
 #pragma unroll
@@ -60,108 +91,114 @@ __device__ __forceinline__ bool in_grid(const Geo &g, const int *c) {
 }
 
 // Fluxes along dir with reciprocal arithmetic (the same physical fluxes as
-// fluxes_at): rho, momentum, energy, induction.
-template <int D>
-__device__ __forceinline__ void fluxes_fast(const Cell<D> &c, long long i, int dir, double gam, double *F) {
+// fluxes_at): rho, momentum, energy, induction.  rho_t, its reciprocal and
+// the total pressure are formed in FP64.
+template <int D, typename T>
+__device__ __forceinline__ void fluxes_fast(const CellT<D, T> &c, long long i, int dir, double gam, T *F) {
   using L = Lay<D>;
-  const double rho = c.v(L::RHO, i), rt = rho + c.v(L::RHOB, i);
-  const double irt = 1.0 / rt;
-  double m[D], b[D], bb[D];
+  const T rho = c.v(L::RHO, i);
+  const double rt = (double)rho + c.vd(L::RHOB, i);
+  const double irtd = 1.0 / rt;
+  const T irt = (T)irtd;
+  T m[D], b[D], bb[D];
 #pragma unroll
   for (int k = 0; k < D; ++k) {
     m[k] = c.v(L::M0 + k, i);
     b[k] = c.v(L::B0 + k, i);
     bb[k] = c.v(L::BB0 + k, i);
   }
-  const double e = c.v(L::EN, i), eb = c.v(L::EB, i);
-  double bbb = 0, b2 = 0, m2 = 0, bbm = 0, bm = 0;
+  const T e = c.v(L::EN, i), eb = c.v(L::EB, i);
+  double bbb = 0, b2 = 0, m2 = 0;
+  T bbm = 0, bm = 0;
 #pragma unroll
   for (int k = 0; k < D; ++k) {
-    bbb += b[k] * bb[k];
-    b2 += b[k] * b[k];
-    m2 += m[k] * m[k];
+    bbb += (double)b[k] * (double)bb[k];
+    b2 += (double)b[k] * (double)b[k];
+    m2 += (double)m[k] * (double)m[k];
     bbm += bb[k] * m[k];
     bm += b[k] * m[k];
   }
-  const double pt = (gam - 1.0) * (e - 0.5 * m2 * irt) - (gam - 2.0) * (bbb + 0.5 * b2);
-  const double md = m[dir], vd = md * irt;
-  const double bd = b[dir], bbd = bb[dir];
+  const T pt = (T)((gam - 1.0) * ((double)e - 0.5 * m2 * irtd) - (gam - 2.0) * (bbb + 0.5 * b2));
+  const T md = m[dir], vd = md * irt;
+  const T bd = b[dir], bbd = bb[dir];
   F[L::RHO] = md;
 #pragma unroll
   for (int k = 0; k < D; ++k) {
-    double f = vd * m[k] - (b[k] * bbd + bb[k] * bd) - b[k] * bd;
+    T f = vd * m[k] - (b[k] * bbd + bb[k] * bd) - b[k] * bd;
     if (k == dir) f += pt;
     F[L::M0 + k] = f;
   }
   F[L::EN] = vd * (e + eb) + (md * pt - bd * bbm - bbd * bm - bd * bm) * irt;
 #pragma unroll
   for (int k = 0; k < D; ++k)
-    F[L::B0 + k] = (k == dir) ? 0.0 : vd * (b[k] + bb[k]) - (bd + bbd) * m[k] * irt;
+    F[L::B0 + k] = (k == dir) ? T(0) : vd * (b[k] + bb[k]) - (bd + bbd) * m[k] * irt;
 }
 
 // q values for the hyperviscosity of all fields of one dimension d:
-// slot 0 rho, 1 internal energy q_e, 2..2+D-1 velocities, then B_f (f != d).
-template <int D>
-__device__ __forceinline__ void q_all(const Cell<D> &c, long long i, int d, double *q) {
+// slot 0 rho, 1 internal energy q_e (formed in FP64), 2..2+D-1 velocities,
+// then B_f (f != d).
+template <int D, typename T>
+__device__ __forceinline__ void q_all(const CellT<D, T> &c, long long i, int d, T *q) {
   using L = Lay<D>;
-  const double rho = c.v(L::RHO, i);
-  const double irt = 1.0 / (rho + c.v(L::RHOB, i));
+  const T rho = c.v(L::RHO, i);
+  const double irtd = 1.0 / ((double)rho + c.vd(L::RHOB, i));
+  const T irt = (T)irtd;
   double b2 = 0, m2 = 0;
   q[0] = rho;
 #pragma unroll
   for (int k = 0; k < D; ++k) {
-    const double m = c.v(L::M0 + k, i), b = c.v(L::B0 + k, i);
-    b2 += b * b;
-    m2 += m * m;
+    const T m = c.v(L::M0 + k, i), b = c.v(L::B0 + k, i);
+    b2 += (double)b * (double)b;
+    m2 += (double)m * (double)m;
     q[2 + k] = m * irt;
   }
-  q[1] = c.v(L::EN, i) - 0.5 * (b2 + m2 * irt);
+  q[1] = (T)(c.vd(L::EN, i) - 0.5 * (b2 + m2 * irtd));
   int s = 2 + D;
 #pragma unroll
   for (int f = 0; f < D; ++f)
     if (f != d) q[s++] = c.v(L::B0 + f, i);
 }
 
-template <int D>
-__global__ void __launch_bounds__(256, 2) tile_stage_kernel(StageArgs a, Geo g, Phys p) {
+// One RK stage on the tile (bx, by, bz) of one simulation; every thread of
+// the block calls it (it synchronises the block).  sm: tile_smem_elems<D, S>()
+// elements of T.
+template <int D, typename T, typename S>
+__device__ __forceinline__ void tile_body(const StageArgs &a, const Geo &g, const Phys &p, int bx, int by, int bz,
+                                          T *sm) {
   using L = Lay<D>;
-  using S = TileShape<D>;
   constexpr int TX = S::TX, TY = S::TY, TZ = S::TZ, NT = TX * TY * TZ;
   constexpr int NW = L::NW, NB = L::NVAR - NW;
   constexpr int NQ = 2 * D + 1;  // q slots per cell for one dimension
-  extern __shared__ double sm[];
+  constexpr bool MIXED = sizeof(T) == sizeof(float);
 
   const int t = threadIdx.x;
   const int tc[3] = {t % TX, (t / TX) % TY, D == 3 ? t / (TX * TY) : 0};
-  const int org[3] = {2 + (int)blockIdx.x * TX, 2 + (int)blockIdx.y * TY, D == 3 ? 2 + (int)blockIdx.z * TZ : 0};
+  const int org[3] = {2 + bx * TX, 2 + by * TY, D == 3 ? 2 + bz * TZ : 0};
   int c[3] = {org[0] + tc[0], org[1] + tc[1], org[2] + tc[2]};
   bool active = true;
 #pragma unroll
   for (int d = 0; d < D; ++d)
     if (c[d] > g.n[d] - 3) active = false;
   const long long idx = active ? gidx<D>(g, c) : 0;
-  const Cell<D> C{a.in, a.bg, g.N};
+  const CellT<D, T> C{MIXED ? (const T *)(const void *)a.in32 : (const T *)(const void *)a.in, a.bg, g.N};
   const double dt = a.sc->dt;
   const double h = dt / a.hdiv;
-  double cm[3] = {0, 0, 0};
+  T cm[3] = {0, 0, 0};
 #pragma unroll
-  for (int d = 0; d < D; ++d) cm[d] = red_get(a.sc->red[a.red_in], d);
+  for (int d = 0; d < D; ++d) cm[d] = (T)red_get(a.sc->red[a.red_in], d);
   int tile_ext[3] = {TX, TY, D == 3 ? TZ : 1};
-  double idx1[3] = {0, 0, 0}, dxc[3] = {1, 1, 1};
+  T idx1[3] = {0, 0, 0};
   if (active) {
 #pragma unroll
-    for (int d = 0; d < D; ++d) {
-      dxc[d] = __ldg(g.dx1[d] + c[d]);
-      idx1[d] = 1.0 / dxc[d];
-    }
+    for (int d = 0; d < D; ++d) idx1[d] = (T)(1.0 / __ldg(g.dx1[d] + c[d]));
   }
-  double dL[NW];
+  T dL[NW];
 #pragma unroll
-  for (int f = 0; f < NW; ++f) dL[f] = 0.0;
-  double numax = 0.0;
+  for (int f = 0; f < NW; ++f) dL[f] = 0;
+  T numax = 0;
 
   // ------------------------------------------------ flux divergences
-#pragma unroll 1
+#pragma unroll
   for (int dir = 0; dir < D; ++dir) {
     TileBox<D> box;
 #pragma unroll
@@ -173,12 +210,12 @@ __global__ void __launch_bounds__(256, 2) tile_stage_kernel(StageArgs a, Geo g, 
     for (int r = t; r < nbox; r += NT) {
       int cc[3];
       box.at(r, cc);
-      double F[NW];
+      T F[NW];
       if (in_grid<D>(g, cc)) {
-        fluxes_fast<D>(C, gidx<D>(g, cc), dir, p.gamma, F);
+        fluxes_fast<D, T>(C, gidx<D>(g, cc), dir, p.gamma, F);
       } else {
 #pragma unroll
-        for (int f = 0; f < NW; ++f) F[f] = 0.0;
+        for (int f = 0; f < NW; ++f) F[f] = 0;
       }
 #pragma unroll
       for (int f = 0; f < NW; ++f) sm[f * nbox + r] = F[f];
@@ -189,11 +226,11 @@ __global__ void __launch_bounds__(256, 2) tile_stage_kernel(StageArgs a, Geo g, 
       int cc[3] = {c[0], c[1], c[2]};
       const int r0 = box.index(cc);
       const int st = dir == 0 ? 1 : dir == 1 ? box.ext[0] : box.ext[0] * box.ext[1];
-      const double w12 = idx1[dir] * (1.0 / 12.0);
+      const T w12 = idx1[dir] * (T)(1.0 / 12.0);
 #pragma unroll
       for (int f = 0; f < NW; ++f) {
-        const double *Fp = sm + f * nbox + r0;
-        double gr = (8.0 * (Fp[st] - Fp[-st]) - (Fp[2 * st] - Fp[-2 * st])) * w12;
+        const T *Fp = sm + f * nbox + r0;
+        T gr = ((T)8 * (Fp[st] - Fp[-st]) - (Fp[2 * st] - Fp[-2 * st])) * w12;
         if (!zr) dL[f] -= gr;
       }
     }
@@ -202,16 +239,16 @@ __global__ void __launch_bounds__(256, 2) tile_stage_kernel(StageArgs a, Geo g, 
 
   // ------------------------------------------------ gravity
   if (active && p.has_grav) {
-    const double rho = C.v(L::RHO, idx), irt = 1.0 / (rho + C.v(L::RHOB, idx));
+    const T rho = C.v(L::RHO, idx), irt = (T)(1.0 / ((double)rho + C.vd(L::RHOB, idx)));
 #pragma unroll
     for (int k = 0; k < D; ++k) {
-      dL[L::M0 + k] += p.g[k] * rho;
-      dL[L::EN] += rho * p.g[k] * C.v(L::M0 + k, idx) * irt;
+      dL[L::M0 + k] += (T)p.g[k] * rho;
+      dL[L::EN] += rho * (T)p.g[k] * C.v(L::M0 + k, idx) * irt;
     }
   }
 
   // ------------------------------------------------ per-dimension hyperdiffusion
-#pragma unroll 1
+#pragma unroll
   for (int d = 0; d < D; ++d) {
     if (!p.hyperdif && !p.has_bgb) break;
     // q box: tile widened by 3 along d and 1 across
@@ -232,12 +269,12 @@ __global__ void __launch_bounds__(256, 2) tile_stage_kernel(StageArgs a, Geo g, 
       nb.ext[e] = tile_ext[e] + 2 * w;
     }
     const int nn = nb.size();
-    double *Q = sm;             // [NQ][nq]
-    double *NU = sm + NQ * nq;  // [2*NQ][nn]: nu_R, nu_L per q slot
+    T *Q = sm;             // [NQ][nq]
+    T *NU = sm + NQ * nq;  // [2*NQ][nn]: nu_R, nu_L per q slot
     for (int r = t; r < nq; r += NT) {
       int cc[3];
       qb.at(r, cc);
-      double q[NQ];
+      T q[NQ];
       const int x = cc[d];
       bool ok = true;
 #pragma unroll
@@ -245,11 +282,11 @@ __global__ void __launch_bounds__(256, 2) tile_stage_kernel(StageArgs a, Geo g, 
         if (e != d && (cc[e] < 0 || cc[e] >= g.n[e])) ok = false;
       if (!ok || x >= g.n[d]) {  // x == n: right pad of the padded q copy (0)
 #pragma unroll
-        for (int k = 0; k < NQ; ++k) q[k] = 0.0;
+        for (int k = 0; k < NQ; ++k) q[k] = 0;
       } else {
         int src[3] = {cc[0], cc[1], cc[2]};
         if (x < 0) src[d] = 5;  // left pad: q(-1) = q(5)
-        q_all<D>(C, gidx<D>(g, src), d, q);
+        q_all<D, T>(C, gidx<D>(g, src), d, q);
       }
 #pragma unroll
       for (int k = 0; k < NQ; ++k) Q[k * nq + r] = q[k];
@@ -264,40 +301,40 @@ __global__ void __launch_bounds__(256, 2) tile_stage_kernel(StageArgs a, Geo g, 
 #pragma unroll
         for (int e = 0; e < D; ++e)
           if (cc[e] < 2 || cc[e] > g.n[e] - 3) inner = false;
-        double nr[NQ], nl[NQ];
+        T nr[NQ], nl[NQ];
 #pragma unroll
         for (int k = 0; k < NQ; ++k) {
-          nr[k] = 0.0;
-          nl[k] = 0.0;
+          nr[k] = 0;
+          nl[k] = 0;
         }
         if (inner) {
           const int rq = qb.index(cc);
-          const double dxd = __ldg(g.dx1[d] + cc[d]);
+          const T dxd = (T)__ldg(g.dx1[d] + cc[d]);
 #pragma unroll
           for (int k = 0; k < NQ; ++k) {
-            const double *qq = Q + k * nq + rq;
-            double qv[7];
+            const T *qq = Q + k * nq + rq;
+            T qv[7];
 #pragma unroll
             for (int o = -3; o <= 3; ++o) qv[o + 3] = qq[o * sd];
-            double m3r = 0, m1r = 0, m3l = 0, m1l = 0;
+            T m3r = 0, m1r = 0, m3l = 0, m1l = 0;
 #pragma unroll
             for (int s2 = -1; s2 <= 1; ++s2) {
-              m3r = fmax(m3r, fabs(3.0 * (qv[s2 + 4] - qv[s2 + 3]) - (qv[s2 + 5] - qv[s2 + 2])));
-              m3l = fmax(m3l, fabs(3.0 * (qv[s2 + 3] - qv[s2 + 2]) - (qv[s2 + 4] - qv[s2 + 1])));
+              m3r = vmax(m3r, vabs((T)3 * (qv[s2 + 4] - qv[s2 + 3]) - (qv[s2 + 5] - qv[s2 + 2])));
+              m3l = vmax(m3l, vabs((T)3 * (qv[s2 + 3] - qv[s2 + 2]) - (qv[s2 + 4] - qv[s2 + 1])));
             }
 #pragma unroll
             for (int s2 = -2; s2 <= 2; ++s2) {
-              m1r = fmax(m1r, fabs(qv[s2 + 4] - qv[s2 + 3]));
-              m1l = fmax(m1l, fabs(qv[s2 + 3] - qv[s2 + 2]));
+              m1r = vmax(m1r, vabs(qv[s2 + 4] - qv[s2 + 3]));
+              m1l = vmax(m1l, vabs(qv[s2 + 3] - qv[s2 + 2]));
             }
             int fid = k == 0 ? L::RHO : k == 1 ? L::EN : k < 2 + D ? L::M0 + (k - 2) : 0;
             if (k >= 2 + D) {
               const int ff = k - (2 + D);
               fid = L::B0 + (ff >= d ? ff + 1 : ff);
             }
-            const double kk = dxd * cm[d] * p.chyp[fid];
-            nr[k] = m1r > 0 ? kk * m3r / m1r : 0.0;
-            nl[k] = m1l > 0 ? kk * m3l / m1l : 0.0;
+            const T kk = dxd * cm[d] * (T)p.chyp[fid];
+            nr[k] = m1r > 0 ? kk * m3r / m1r : T(0);
+            nl[k] = m1l > 0 ? kk * m3l / m1l : T(0);
           }
         }
 #pragma unroll
@@ -314,51 +351,51 @@ __global__ void __launch_bounds__(256, 2) tile_stage_kernel(StageArgs a, Geo g, 
       const int n0 = nb.index(cc);
       const long long sg = g.st[d];
       const bool zd = z1(g, c, d);
-      const double i1 = idx1[d], i2 = idx1[d] * idx1[d];
+      const T i1 = idx1[d], i2 = idx1[d] * idx1[d];
       if (p.has_bgb) {  // background energy terms along d (addenergyterms_cd2)
         double bb2 = 0;
 #pragma unroll
-        for (int k = 0; k < D; ++k) bb2 += C.v(L::BB0 + k, idx) * C.v(L::BB0 + k, idx);
-        const double ptb = (p.gamma - 1) * C.v(L::EB, idx) - 0.5 * (p.gamma - 2) * bb2;
+        for (int k = 0; k < D; ++k) bb2 += C.vd(L::BB0 + k, idx) * C.vd(L::BB0 + k, idx);
+        const T ptb = (T)((p.gamma - 1) * C.vd(L::EB, idx) - 0.5 * (p.gamma - 2) * bb2);
         const bool z4d = z4(g, c, d);
 #pragma unroll
         for (int dir = 0; dir < D; ++dir) {
-          const double *v = Q + (2 + dir) * nq + r0;
-          double gv = z4d ? 0.0 : (8.0 * (v[sd] - v[-sd]) - (v[2 * sd] - v[-2 * sd])) * (i1 * (1.0 / 12.0));
+          const T *v = Q + (2 + dir) * nq + r0;
+          T gv = z4d ? T(0) : ((T)8 * (v[sd] - v[-sd]) - (v[2 * sd] - v[-2 * sd])) * (i1 * (T)(1.0 / 12.0));
           if (d == dir) dL[L::EN] -= ptb * gv;
           dL[L::EN] += C.v(L::BB0 + d, idx) * C.v(L::BB0 + dir, idx) * gv;
         }
       }
       if (p.hyperdif) {
 #pragma unroll
-        for (int k = 0; k < NQ; ++k) numax = fmax(numax, fmax(NU[2 * k * nn + n0], NU[(2 * k + 1) * nn + n0]));
+        for (int k = 0; k < NQ; ++k) numax = vmax(numax, vmax(NU[2 * k * nn + n0], NU[(2 * k + 1) * nn + n0]));
         // rho and internal energy: f += (nu_R dq+ - nu_L dq-) / dx^2
 #pragma unroll
         for (int k = 0; k < 2; ++k) {
-          const double *q = Q + k * nq + r0;
-          const double nr = NU[2 * k * nn + n0], nl = NU[(2 * k + 1) * nn + n0];
-          const double dp = zd ? 0.0 : q[sd] - q[0], dm = zd ? 0.0 : q[0] - q[-sd];
+          const T *q = Q + k * nq + r0;
+          const T nr = NU[2 * k * nn + n0], nl = NU[(2 * k + 1) * nn + n0];
+          const T dp = zd ? T(0) : q[sd] - q[0], dm = zd ? T(0) : q[0] - q[-sd];
           dL[k == 0 ? L::RHO : L::EN] += (nr * dp - nl * dm) * i2;
         }
         // momentum
-        const double rt0 = C.v(L::RHO, idx) + C.v(L::RHOB, idx);
-        const double rtp = C.v(L::RHO, idx + sg) + C.v(L::RHOB, idx + sg);
-        const double rtm = C.v(L::RHO, idx - sg) + C.v(L::RHOB, idx - sg);
+        const T rt0 = C.v(L::RHO, idx) + C.v(L::RHOB, idx);
+        const T rtp = C.v(L::RHO, idx + sg) + C.v(L::RHOB, idx + sg);
+        const T rtm = C.v(L::RHO, idx - sg) + C.v(L::RHOB, idx - sg);
 #pragma unroll
         for (int f = 0; f < D; ++f) {
           const int k = 2 + f;
-          const double *v = Q + k * nq + r0;
-          const double nr = NU[2 * k * nn + n0], nl = NU[(2 * k + 1) * nn + n0];
-          const double dvp = zd ? 0.0 : v[sd] - v[0], dvm = zd ? 0.0 : v[0] - v[-sd];
-          const double m0 = C.v(L::M0 + f, idx), mp = C.v(L::M0 + f, idx + sg), mm = C.v(L::M0 + f, idx - sg);
-          const double fac = (f == d ? 1.0 : 0.5) * i2;
-          dL[L::M0 + f] += ((rt0 + rtp) * nr * dvp - (rt0 + rtm) * nl * dvm) * 0.5 * fac;
-          dL[L::EN] += ((m0 + mp) * nr * dvp - (m0 + mm) * nl * dvm) * 0.5 * fac;
+          const T *v = Q + k * nq + r0;
+          const T nr = NU[2 * k * nn + n0], nl = NU[(2 * k + 1) * nn + n0];
+          const T dvp = zd ? T(0) : v[sd] - v[0], dvm = zd ? T(0) : v[0] - v[-sd];
+          const T m0 = C.v(L::M0 + f, idx), mp = C.v(L::M0 + f, idx + sg), mm = C.v(L::M0 + f, idx - sg);
+          const T fac = (f == d ? (T)1 : (T)0.5) * i2;
+          dL[L::M0 + f] += ((rt0 + rtp) * nr * dvp - (rt0 + rtm) * nl * dvm) * (T)0.5 * fac;
+          dL[L::EN] += ((m0 + mp) * nr * dvp - (m0 + mm) * nl * dvm) * (T)0.5 * fac;
           if (f != d) {  // off-diagonal: m_d += d_f( rho_t (nu_R+nu_L)/4 d_d v_f )
             const int sf = f == 0 ? 1 : f == 1 ? qb.ext[0] : qb.ext[0] * qb.ext[1];
             const int nf = f == 0 ? 1 : f == 1 ? nb.ext[0] : nb.ext[0] * nb.ext[1];
             const long long gf = g.st[f];
-            double t1[2], t2[2];
+            T t1[2], t2[2];
 #pragma unroll
             for (int s = 0; s < 2; ++s) {
               const int o = s ? sf : -sf;
@@ -366,14 +403,14 @@ __global__ void __launch_bounds__(256, 2) tile_stage_kernel(StageArgs a, Geo g, 
               const long long go = s ? gf : -gf;
               int cx[3] = {c[0], c[1], c[2]};
               cx[f] += s ? 1 : -1;
-              const double nsum = NU[2 * k * nn + n0 + on] + NU[(2 * k + 1) * nn + n0 + on];
-              const double tmp5 = z1(g, cx, d) ? 0.0 : (v[o + sd] - v[o - sd]) * 0.5 * i1;
-              const double tmp6 = tmp5 * nsum * 0.25;
+              const T nsum = NU[2 * k * nn + n0 + on] + NU[(2 * k + 1) * nn + n0 + on];
+              const T tmp5 = z1(g, cx, d) ? T(0) : (v[o + sd] - v[o - sd]) * (T)0.5 * i1;
+              const T tmp6 = tmp5 * nsum * (T)0.25;
               t1[s] = (C.v(L::RHO, idx + go) + C.v(L::RHOB, idx + go)) * tmp6;
               t2[s] = tmp6 * C.v(L::M0 + d, idx + go);
             }
             const bool zf = z1(g, c, f);
-            const double hf = 0.5 * idx1[f];
+            const T hf = (T)0.5 * idx1[f];
             if (!zf) {
               dL[L::M0 + d] += (t1[1] - t1[0]) * hf;
               dL[L::EN] += (t2[1] - t2[0]) * hf;
@@ -386,13 +423,13 @@ __global__ void __launch_bounds__(256, 2) tile_stage_kernel(StageArgs a, Geo g, 
         for (int f = 0; f < D; ++f) {
           if (f == d) continue;
           const int k = ks++;
-          const double *b = Q + k * nq + r0;
-          const double nr = NU[2 * k * nn + n0], nl = NU[(2 * k + 1) * nn + n0];
+          const T *b = Q + k * nq + r0;
+          const T nr = NU[2 * k * nn + n0], nl = NU[(2 * k + 1) * nn + n0];
           {  // off-diagonal: B_d -= d_f( (nu_L+nu_R)/2 d_d B_f ), e likewise with B_d
             const int sf = f == 0 ? 1 : f == 1 ? qb.ext[0] : qb.ext[0] * qb.ext[1];
             const int nf = f == 0 ? 1 : f == 1 ? nb.ext[0] : nb.ext[0] * nb.ext[1];
             const long long gf = g.st[f];
-            double t1[2], t2[2];
+            T t1[2], t2[2];
 #pragma unroll
             for (int s = 0; s < 2; ++s) {
               const int o = s ? sf : -sf;
@@ -400,21 +437,21 @@ __global__ void __launch_bounds__(256, 2) tile_stage_kernel(StageArgs a, Geo g, 
               const long long go = s ? gf : -gf;
               int cx[3] = {c[0], c[1], c[2]};
               cx[f] += s ? 1 : -1;
-              const double nsum = NU[2 * k * nn + n0 + on] + NU[(2 * k + 1) * nn + n0 + on];
-              const double tmp2 = z1(g, cx, d) ? 0.0 : (b[o + sd] - b[o - sd]) * 0.5 * i1;
-              t1[s] = tmp2 * nsum * 0.5;
+              const T nsum = NU[2 * k * nn + n0 + on] + NU[(2 * k + 1) * nn + n0 + on];
+              const T tmp2 = z1(g, cx, d) ? T(0) : (b[o + sd] - b[o - sd]) * (T)0.5 * i1;
+              t1[s] = tmp2 * nsum * (T)0.5;
               t2[s] = t1[s] * C.v(L::B0 + d, idx + go);
             }
             if (!z1(g, c, f)) {
-              const double hf = 0.5 * idx1[f];
+              const T hf = (T)0.5 * idx1[f];
               dL[L::B0 + d] -= (t1[1] - t1[0]) * hf;
               dL[L::EN] -= (t2[1] - t2[0]) * hf;
             }
           }
           {  // diagonal: B_f += (nu_R dB+ - nu_L dB-)/dx^2 and Ohmic heating
-            const double dbp = zd ? 0.0 : b[sd] - b[0], dbm = zd ? 0.0 : b[0] - b[-sd];
+            const T dbp = zd ? T(0) : b[sd] - b[0], dbm = zd ? T(0) : b[0] - b[-sd];
             dL[L::B0 + f] += (nr * dbp - nl * dbm) * i2;
-            dL[L::EN] += (0.5 * (b[0] + b[sd]) * nr * dbp - 0.5 * (b[0] + b[-sd]) * nl * dbm) * i2;
+            dL[L::EN] += ((T)0.5 * (b[0] + b[sd]) * nr * dbp - (T)0.5 * (b[0] + b[-sd]) * nl * dbm) * i2;
           }
         }
       }
@@ -423,50 +460,99 @@ __global__ void __launch_bounds__(256, 2) tile_stage_kernel(StageArgs a, Geo g, 
   }
 
   // ------------------------------------------------ combine, write, reduce
-  double red[6] = {0, 0, 0, 0, 0, numax};
+  double red[6] = {0, 0, 0, 0, 0, (double)numax};
   if (active) {
     double o[NW];
+    float hi[NW], lo[NW];
+    if (!MIXED) {
 #pragma unroll
-    for (int f = 0; f < NW; ++f) o[f] = a.base[(long long)f * g.N + idx] + h * dL[f];
-    if (a.kind == 3) {
+      for (int f = 0; f < NW; ++f) o[f] = a.base[(long long)f * g.N + idx] + h * (double)dL[f];
+      if (a.kind == 3) {
+#pragma unroll
+        for (int f = 0; f < NW; ++f) {
+          const long long j = (long long)f * g.N + idx;
+          a.acc[j] = (a.acc[j] + 2.0 * C.vd(f, idx) + o[f] - 4.0 * a.base[j]) * (1.0 / 3.0);
+        }
+      } else if (a.kind == 4) {
+#pragma unroll
+        for (int f = 0; f < NW; ++f) o[f] += a.acc[(long long)f * g.N + idx];
+      }
+    } else {
+      // RK4 in increment form, W = w32 + c32:
+      //   stages k = 1..3: S_k = W + h_k L_k (FP32), A += c_k h_k L_k with
+      //   c = 1/3, 2/3, 1/3, so A = (S1 + 2 S2 + S3 - 4 W) / 3 as the FP64 path;
+      //   stage 4: W <- W + h_4 L_4 + A, kept as value + compensation.
+      // Stages 1..3 round to FP32 anyway, so they take the base without c32.
 #pragma unroll
       for (int f = 0; f < NW; ++f) {
         const long long j = (long long)f * g.N + idx;
-        a.acc[j] = (a.acc[j] + 2.0 * C.v(f, idx) + o[f] - 4.0 * a.base[j]) * (1.0 / 3.0);
+        const double inc = h * (double)dL[f];
+        if (a.kind == 4) {
+          const double wn = ((double)a.w32[j] + (double)a.c32[j]) + (inc + (double)a.acc32[j]);
+          hi[f] = (float)wn;
+          lo[f] = (float)(wn - (double)hi[f]);
+        } else {
+          hi[f] = (float)((double)a.w32[j] + inc);
+          const double prev = a.kind == 1 ? 0.0 : (double)a.acc32[j];
+          a.acc32[j] = (float)(prev + (a.kind == 2 ? 2.0 : 1.0) * (1.0 / 3.0) * inc);
+        }
+        o[f] = (double)hi[f];  // what the next stage reads
       }
-    } else if (a.kind == 4) {
-#pragma unroll
-      for (int f = 0; f < NW; ++f) o[f] += a.acc[(long long)f * g.N + idx];
     }
-    int xs[3][2], nx[3];
+    // the cell and its ghost images: per dim the own coordinate and, at most,
+    // one image coordinate (images()), combined over all dims
+    int x0[3], x1[3], has[3];
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
-      if (d < D)
-        nx[d] = images(g, d, c[d], xs[d]);
-      else {
-        nx[d] = 1;
-        xs[d][0] = 0;
-      }
+      int xs[2] = {0, 0};
+      has[d] = d < D ? (images(g, d, c[d], xs) == 2) : 0;
+      x0[d] = d < D ? c[d] : 0;
+      x1[d] = xs[1];
     }
-    for (int iz = 0; iz < nx[2]; ++iz)
-      for (int iy = 0; iy < nx[1]; ++iy)
-        for (int ix = 0; ix < nx[0]; ++ix) {
-          const long long j = xs[0][ix] + (long long)xs[1][iy] * g.st[1] + (D == 3 ? (long long)xs[2][iz] * g.st[2] : 0);
 #pragma unroll
-          for (int f = 0; f < NW; ++f) a.out[(long long)f * g.N + j] = o[f];
-          double bgv[NB];
+    for (int m = 0; m < (1 << D); ++m) {
+      bool ok = true;
+      int cc[3];
 #pragma unroll
-          for (int b = 0; b < NB; ++b) bgv[b] = __ldg(a.bg + (long long)b * g.N + j);
-          reduce_cell<D>(g, p, o, bgv, j, red);
+      for (int d = 0; d < 3; ++d) {
+        const bool b = d < D && ((m >> d) & 1);
+        if (b && !has[d]) ok = false;
+        cc[d] = b ? x1[d] : x0[d];
+      }
+      if (!ok) continue;
+      const long long j = gidx<D>(g, cc);
+      if (!MIXED) {
+#pragma unroll
+        for (int f = 0; f < NW; ++f) a.out[(long long)f * g.N + j] = o[f];
+      } else if (a.kind == 4) {
+#pragma unroll
+        for (int f = 0; f < NW; ++f) {
+          a.w32[(long long)f * g.N + j] = hi[f];
+          a.c32[(long long)f * g.N + j] = lo[f];
         }
+      } else {
+#pragma unroll
+        for (int f = 0; f < NW; ++f) a.out32[(long long)f * g.N + j] = hi[f];
+      }
+      double bgv[NB];
+#pragma unroll
+      for (int b = 0; b < NB; ++b) bgv[b] = __ldg(a.bg + (long long)b * g.N + j);
+      reduce_cell<D>(g, p, o, bgv, j, red);
+    }
   }
   block_max_flush<6>(red, &a.sc->red[a.red_out]);
 }
 
-// shared memory bytes the tile kernel needs
-template <int D>
-__host__ __device__ constexpr int tile_smem_doubles() {
-  using S = TileShape<D>;
+// One launch = one RK stage of one simulation, one block per tile.
+template <int D, typename T>
+__global__ void __launch_bounds__(256, 2) tile_stage_kernel(StageArgs a, Geo g, Phys p) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  tile_body<D, T, TileShape<D>>(a, g, p, blockIdx.x, blockIdx.y, blockIdx.z, reinterpret_cast<T *>(smraw));
+}
+
+// shared memory elements (of the stencil type) the tile body needs
+template <int D, typename S = TileShape<D>>
+__host__ __device__ constexpr int tile_smem_elems() {
   constexpr int NW = 2 + 2 * D, NQ = 2 * D + 1;
   constexpr int ex[3] = {S::TX, S::TY, D == 3 ? S::TZ : 1};
   // flux box, largest over dir

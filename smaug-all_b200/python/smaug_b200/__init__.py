@@ -27,7 +27,11 @@ SMAUG_OK = 0
 class Params(ctypes.Structure):
     _fields_ = [("ndim", _I), ("n", _I * 3), ("gamma", _D), ("courant", _D), ("chyp", _D * 13),
                 ("btype", _I * 3), ("g", _D * 3), ("hyperdif", _I), ("rk4", _I), ("dt_mode", _I),
-                ("dt0", _D), ("exact", _I)]
+                ("dt0", _D), ("exact", _I), ("precision", _I)]
+
+
+PREC_FP64 = 0   # SMAUG_PREC_FP64
+PREC_MIXED = 1  # SMAUG_PREC_MIXED: FP32 stage states and stencils, FP64 where accuracy needs it
 
 
 class SmaugError(RuntimeError):
@@ -77,7 +81,7 @@ class Engine:
     """One simulation resident on one GPU."""
 
     def __init__(self, prob, rk4: bool = True, dt_mode: int = 1, exact: bool = False, device: int = 0,
-                 dt0: float = 0.0):
+                 dt0: float = 0.0, precision: int = PREC_FP64):
         self.lib = load_library()
         self.prob = prob
         p = Params()
@@ -95,6 +99,7 @@ class Engine:
         p.dt_mode = int(dt_mode)
         p.dt0 = float(dt0)
         p.exact = int(exact)
+        p.precision = int(precision)
         self.params = p
         h = ctypes.c_void_p()
         rc = self.lib.smaug_create(ctypes.byref(p), device, ctypes.byref(h))

@@ -57,3 +57,25 @@ def test_create_rejects_bad_arguments():
     h = ctypes.c_void_p()
     assert lib.smaug_create(ctypes.byref(p), 0, ctypes.byref(h)) == -1
     lib.smaug_destroy(h)
+
+
+def test_create_rejects_bad_precision():
+    """Parameter checks run before any CUDA call, so they need no GPU."""
+    from smaug_b200 import PREC_MIXED, Params
+    lib = load_library()
+    lib.smaug_last_error.restype = ctypes.c_char_p
+    p = Params()
+    p.ndim = 2
+    p.n[0], p.n[1], p.n[2] = 20, 20, 1
+    p.rk4 = 1
+    p.precision = 7
+    h = ctypes.c_void_p()
+    assert lib.smaug_create(ctypes.byref(p), 0, ctypes.byref(h)) == -1
+    assert b"precision" in lib.smaug_last_error(h)
+    lib.smaug_destroy(h)
+    for rk4, exact in [(0, 0), (1, 1)]:
+        p.precision, p.rk4, p.exact = PREC_MIXED, rk4, exact
+        h = ctypes.c_void_p()
+        assert lib.smaug_create(ctypes.byref(p), 0, ctypes.byref(h)) == -1
+        assert b"mixed" in lib.smaug_last_error(h)
+        lib.smaug_destroy(h)
