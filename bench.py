@@ -1,18 +1,21 @@
 #!/usr/bin/env python3
-"""Benchmark: ideal-MHD cell-updates/s on B200 (SAC/SMAUG method).
+"""Benchmark: ideal-MHD cell-updates/s on B200 (SAC/SMAUG method), batched
+mixed precision against the plain FP64 single-simulation path.
 
-Workload (one step = one full RK4 step of the whole grid): the 3-D blast wave,
-128^3 interior cells (+2 ghost layers), periodic, hyperdiffusion on, Courant
-0.3 with the reference's dt rule; seeded synthetic initial state.  The
-headline line runs the mixed-precision path (FP32 stage states and stencils,
-FP64 backgrounds, pressure / internal-energy recovery, RK base and sum, dt);
-the plain FP64 path is measured beside it on the same workload ("companion")
-and the two final states are compared ("accuracy").
+Headline workload (one step = one full RK4 step of every simulation): the
+batched ensemble of 96 independent 2-D Orszag-Tang vortices, sides drawn from
+{128, 192, 256, 384, 512, 768} (seed 4242), B0 scaled by U[0.5, 1.5], 1 %
+density noise, hyperdiffusion on, each with its own dt from the reference's
+rule.  `value` is the batch (all 96 in one launch per RK stage, CUDA graphs,
+mixed precision: FP32 stage states and stencils, FP64 backgrounds, pressure /
+internal-energy recovery, RK base and sum, dt); "plain_fp64" times the same
+96 simulations one after another through the FP64 single-simulation context.
+The 3-D blast wave (128^3, FP64 and mixed, with an accuracy study against the
+FP64 oracle build) is measured beside it ("blast128").
 With --gpus N (torchrun) every rank advances its own replica (no data-path
-collective: independent instances), so scaling is weak.
+collective: independent simulations), so scaling is weak.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                  [--precision mixed|fp64]
 
 --impl reference times the reference's own CPU implementation (the SMAUG
 sources built for the host, oracle/_ref) on a bounded sample of the same
@@ -32,14 +35,18 @@ ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 sys.path.insert(0, str(ROOT / "smaug-all_b200" / "python"))
 
-METRIC = "cell-updates/s (3-D blast wave 128^3, RK4; mixed FP32/FP64 vs plain FP64)"
+METRIC = "cell-updates/s: batched mixed-prec vs plain FP64, 1 B200; p50/p99 latency"
 UNIT = "cell-updates/s"
 # algorithmic HBM bytes per cell-update (one cell, one full RK4 step), 3-D:
 # FP64: 14 evolved-field passes x 8 fields x 8 B + 4 background passes x 5 x 8 B
 BYTES_PER_CELL_UPDATE_FP64_3D = (14 * 8 + 4 * 5) * 8  # 1056 B
 # mixed: 19 FP32 evolved-field passes x 8 fields x 4 B + 4 FP64 background passes
 BYTES_PER_CELL_UPDATE_MIXED_3D = 19 * 8 * 4 + 4 * 5 * 8  # 768 B
-SAMPLE_N = 24          # CPU sample: 24^3 interior cells per process
+# 2-D (6 evolved fields, 4 backgrounds): FP64 800 B, mixed 584 B
+BYTES_PER_CELL_UPDATE_FP64_2D = (14 * 6 + 4 * 4) * 8
+BYTES_PER_CELL_UPDATE_MIXED_2D = 19 * 6 * 4 + 4 * 4 * 8
+ENSEMBLE = {"count": 96, "seed": 4242}
+SAMPLE_N = 128         # CPU sample: one 128^2 Orszag-Tang simulation of the ensemble per process
 SAMPLE_SUBSTEPS = 4    # reference single steps per RK4-equivalent step
 
 
@@ -65,14 +72,14 @@ def load_traffic():
 # ----------------------------------------------------------------- CPU side
 
 def _cpu_worker(args):
-    n, substeps, nsteps, warmup, use_ref = args
+    n, substeps, nsteps, warmup, use_ref, rank = args
     # the reference's host code prints progress on stdout; keep the bench's
     # stdout to its one JSON line
     devnull = os.open(os.devnull, os.O_WRONLY)
     os.dup2(devnull, 1)
-    import numpy as np  # noqa: F401
     from smaug_b200 import problems
-    prob = problems.blast_wave(n)
+    cfg = ENSEMBLE
+    prob = problems.orszag_tang(n, b0_scale=1.0, rho_noise=0.01, seed=cfg["seed"] + rank)
     if use_ref:
         from oracle.oracle import Reference
         sim = Reference(prob)
@@ -92,21 +99,21 @@ def _cpu_worker(args):
 def cpu_throughput(nsteps: int, warmup: int = 1, procs: int | None = None):
     """Cell-updates/s of the reference's CPU code on the host cores."""
     import multiprocessing as mp
-    use_ref = (ROOT / "oracle" / "_ref" / "libsmaug_ref3d.so").exists()
+    use_ref = (ROOT / "oracle" / "_ref" / "libsmaug_ref2d.so").exists()
     procs = procs or os.cpu_count() or 1
     ctx = mp.get_context("spawn")
     substeps = SAMPLE_SUBSTEPS if use_ref else 1
     t0 = time.perf_counter()
     with ctx.Pool(procs) as pool:
-        times = pool.map(_cpu_worker, [(SAMPLE_N, substeps, nsteps, warmup, use_ref)] * procs)
+        times = pool.map(_cpu_worker, [(SAMPLE_N, substeps, nsteps, warmup, use_ref, r) for r in range(procs)])
     wall = time.perf_counter() - t0
     elapsed = max(times)
-    cells = SAMPLE_N ** 3
+    cells = SAMPLE_N ** 2
     value = procs * cells * nsteps / elapsed
     kind = "reference" if use_ref else "port"
-    sample = (f"{procs} processes x blast wave {SAMPLE_N}^3 x {nsteps} RK4-equivalent steps "
-              + (f"({substeps} reference single steps each; reference rkon=1 path is not usable)" if use_ref
-                 else "(oracle port, RK4)"))
+    sample = (f"{procs} processes x one {SAMPLE_N}^2 Orszag-Tang simulation of the ensemble x {nsteps} "
+              "RK4-equivalent steps " + (f"({substeps} reference single steps each; the reference's rkon=1 path "
+                                         "is not usable)" if use_ref else "(oracle port, RK4)"))
     return {"value": value, "unit": UNIT, "cores": procs, "kind": kind, "sample": sample,
             "elapsed_s": elapsed, "wall_s": wall}
 
@@ -121,7 +128,7 @@ def run_reference(a):
             "warmup": a.warmup, "ms_per_step": cpu["elapsed_s"] * 1e3 / max(1, a.steps),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic",
-            "config": dict(workload_config(a.n, a.gpus), precision="fp64 (the reference computes in FP64 only)"),
+            "config": dict(workload_config(a.gpus), precision="fp64 (the reference computes in FP64 only)"),
             "impl": "reference",
             "cpu_baseline": {"value": cpu["value"], "unit": UNIT, "cores": cpu["cores"], "kind": cpu["kind"],
                              "sample": cpu["sample"]},
@@ -130,13 +137,13 @@ def run_reference(a):
     return 0
 
 
-def workload_config(n: int, world: int, ncells: int | None = None):
-    ncells = ncells or (n + 4) ** 3
-    return {"workload": f"blast wave 3-D {n}^3 interior, periodic, RK4, hyperdiffusion on",
-            "ndim": 3, "interior": [n] * 3, "cells_with_ghosts": ncells,
+def workload_config(world: int, cells: int | None = None):
+    return {"workload": "batched ensemble: 96 independent 2-D Orszag-Tang vortices, sides {128..768} "
+                        "(seed 4242), B0 x U[0.5,1.5], 1% density noise, periodic, RK4, hyperdiffusion on, "
+                        "per-simulation dt (reference rule)",
+            "ndim": 2, "simulations": ENSEMBLE["count"], "interior_cells": cells,
             "parallelism": f"replicas x{world}",
-            "l2": f"inputs larger than L2: state 4 x 8 fields x {ncells} x 8 B = "
-                  f"{4 * 8 * ncells * 8 / 1e6:.0f} MB > 126 MB"}
+            "l2": "inputs larger than L2: ensemble state > 1 GB"}
 
 
 # ----------------------------------------------------------------- GPU side
@@ -187,39 +194,161 @@ class ClockSampler:
         return {"sm_mhz": sm[len(sm) // 2], "sm_max_mhz": rows[0][1], "reasons": reasons, "samples": len(rows)}
 
 
-def measure(eng, n_int, steps, warmup, stream, barrier, dist, world, local, sample_clocks):
+def event_ms(stream, fn):
+    """Device time (ms) of the work fn() enqueues on `stream`."""
+    import torch
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    fn()
+    e1.record(stream)
+    e1.synchronize()
+    return e0.elapsed_time(e1)
+
+
+class Ctx:
+    """Ranks, barrier and the max-over-ranks reduction of a time."""
+
+    def __init__(self, a):
+        import torch
+        self.a = a
+        self.rank = int(os.environ.get("RANK", "0"))
+        self.world = int(os.environ.get("WORLD_SIZE", "1"))
+        self.local = int(os.environ.get("LOCAL_RANK", "0"))
+        torch.cuda.set_device(self.local)
+        self.dist = None
+        if self.world > 1:
+            import datetime
+
+            import torch.distributed as dist
+            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+            self.dist = dist
+
+    def barrier(self):
+        if self.dist is not None:
+            self.dist.barrier()
+
+    def max_ms(self, ms: float) -> float:
+        import torch
+        t = torch.tensor([ms], device="cuda")
+        if self.dist is not None:
+            self.dist.all_reduce(t, op=self.dist.ReduceOp.MAX)
+        return float(t.item())
+
+
+def measure(eng, n_int, steps, warmup, ctx, sample_clocks):
     """Device-timed throughput of `steps` full steps of one engine, plus the
     average duration of its stage-kernel launches."""
     import torch
+    stream = torch.cuda.ExternalStream(eng.stream)
     eng.step(max(3, warmup))
     eng.sync()
-    sampler = ClockSampler(local) if sample_clocks else None
+    sampler = ClockSampler(ctx.local) if sample_clocks else None
     if sampler:
         sampler.start()
-    barrier()
+    ctx.barrier()
     torch.cuda.synchronize()
     l0 = eng.launches
-    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    ev0.record(stream)
-    eng.step(steps)
-    ev1.record(stream)
+    ms = event_ms(stream, lambda: eng.step(steps))
     eng.sync()
-    torch.cuda.synchronize()
-    barrier()
+    ctx.barrier()
     clocks = sampler.stop() if sampler else None
-    ms = ev0.elapsed_time(ev1)
     launches = eng.launches - l0
-    t = torch.tensor([ms], device="cuda")
-    if dist is not None:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    ms_max = float(t.item())
-    # per-launch duration of the stage kernel (the dominant kernel)
+    ms_max = ctx.max_ms(ms)
     eng.profile_stages(True)
     eng.step(max(2, min(steps, 8)))
     st_ms, st_n = eng.stage_times()
     eng.profile_stages(False)
-    return {"value": world * n_int * steps / (ms_max / 1e3), "ms_per_step": ms_max / steps,
+    return {"value": ctx.world * n_int * steps / (ms_max / 1e3), "ms_per_step": ms_max / steps,
             "launches": launches, "clocks": clocks, "avg_stage_ms": st_ms / max(st_n, 1)}
+
+
+def run_batched(probs, prec, ctx, steps, warmup, sample_clocks):
+    """The whole ensemble in one batch: tune, warm up, time `steps` steps."""
+    import torch
+
+    from smaug_b200 import Batch, footprint
+    cells = sum(p.interior for p in probs)
+    fp = sum(footprint(p, prec) for p in probs)
+    b = Batch(2, precision=prec, arena_bytes=int(fp * 1.02) + (64 << 20), max_sims=len(probs), device=ctx.local)
+    extra = 64  # steps beyond warm-up, timing and profiling: every simulation stays active throughout
+    for p in probs:
+        if b.add(p, warmup + steps + extra) is None:
+            raise RuntimeError("ensemble does not fit its arena")
+    variant, tune_ms = b.tune(reps=3)
+    stream = torch.cuda.ExternalStream(b.stream)
+    b.step(warmup)
+    b.sync()
+    sampler = ClockSampler(ctx.local) if sample_clocks else None
+    if sampler:
+        sampler.start()
+    ctx.barrier()
+    torch.cuda.synchronize()
+    l0 = b.launches
+    ms = event_ms(stream, lambda: b.step(steps))
+    b.sync()
+    ctx.barrier()
+    clocks = sampler.stop() if sampler else None
+    launches = b.launches - l0
+    ms_max = ctx.max_ms(ms)
+    b.profile_stages(True)
+    b.step(2)
+    st_ms, st_n = b.stage_times()
+    b.profile_stages(False)
+    b.close()
+    return {"value": ctx.world * cells * steps / (ms_max / 1e3), "ms_per_step": ms_max / steps,
+            "launches": launches, "clocks": clocks, "avg_stage_ms": st_ms / max(st_n, 1),
+            "tile_variant": variant, "tune_stage1_ms": tune_ms}
+
+
+def run_plain(probs, prec, ctx, steps, warmup):
+    """The ensemble one simulation after another through the single-simulation
+    context: the sum of their device times for `steps` steps each."""
+    import torch
+
+    from smaug_b200 import Engine
+    cells = sum(p.interior for p in probs)
+    tot = 0.0
+    for p in probs:
+        e = Engine(p, rk4=True, precision=prec, device=ctx.local)
+        stream = torch.cuda.ExternalStream(e.stream)
+        e.step(warmup)
+        e.sync()
+        tot += event_ms(stream, lambda: e.step(steps))
+        e.sync()
+        e.close()
+    ms_max = ctx.max_ms(tot)
+    return {"value": ctx.world * cells * steps / (ms_max / 1e3), "ms_per_step": ms_max / steps}
+
+
+def run_e2e_batched(probs, prec, ctx, steps):
+    """End to end through the public batch API with host buffers: admit every
+    simulation from pinned host memory, advance `steps` steps, read every
+    result back into pinned host memory."""
+    import numpy as np
+    import torch
+
+    from smaug_b200 import Batch, footprint
+    cells = sum(p.interior for p in probs)
+    fp = sum(footprint(p, prec) for p in probs)
+    ins = [torch.from_numpy(np.ascontiguousarray(p.w)).pin_memory() for p in probs]
+    outs = [torch.empty_like(t).pin_memory() for t in ins]
+    b = Batch(2, precision=prec, arena_bytes=int(fp * 1.02) + (64 << 20), max_sims=len(probs), device=ctx.local)
+    stream = torch.cuda.ExternalStream(b.stream)
+    ctx.barrier()
+    torch.cuda.synchronize()
+
+    def job():
+        slots = [b.add(p, steps, w=t.numpy()) for p, t in zip(probs, ins)]
+        b.step(steps)
+        for sl, o in zip(slots, outs):
+            b.state(sl, out=o.numpy())
+
+    ms = event_ms(stream, job)
+    b.close()
+    ms_max = ctx.max_ms(ms)
+    nbytes = sum(t.numel() * 8 for t in ins)
+    return {"value": ctx.world * cells * steps / (ms_max / 1e3), "unit": UNIT,
+            "h2d_bytes_per_step": nbytes / steps, "d2h_bytes_per_step": nbytes / steps}
 
 
 def accuracy_study(prob, steps: int, device: int):
@@ -258,141 +387,133 @@ def accuracy_study(prob, steps: int, device: int):
     return out
 
 
-def main():
-    ap = argparse.ArgumentParser()
-    ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
-    ap.add_argument("--warmup", type=int, default=3)
-    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--n", type=int, default=128, help="interior cells per dim")
-    ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"],
-                    help="arithmetic of the headline line (the other one is measured beside it)")
-    ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--no-companion", action="store_true", help="skip the other precision's measurement")
-    ap.add_argument("--accuracy-steps", type=int, default=50,
-                    help="steps of the accuracy study against the FP64 oracle (0: skip)")
-    a = ap.parse_args()
-    if a.impl == "reference":
-        return run_reference(a)
-
+def run_blast(a, ctx):
+    """3-D blast wave 128^3: mixed and FP64 single simulation, roofline of
+    each, per-step host round trip end to end, accuracy study."""
     import ctypes
 
     import numpy as np
     import torch
 
     from smaug_b200 import PREC_FP64, PREC_MIXED, Engine, problems
-
-    rank = int(os.environ.get("RANK", "0"))
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    torch.cuda.set_device(local)
-    dist = None
-    if world > 1:
-        import datetime
-
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
-
-    def barrier():
-        if dist is not None:
-            dist.barrier()
-
-    prob = problems.blast_wave(a.n, seed=1234 + rank)
+    prob = problems.blast_wave(a.n, seed=1234 + ctx.rank)
     n_int = prob.interior
-    mixed = a.precision == "mixed"
-    prec = PREC_MIXED if mixed else PREC_FP64
-    eng = Engine(prob, rk4=True, exact=False, device=local, precision=prec)
-    stream = torch.cuda.ExternalStream(eng.stream)
+    peak, _ = load_peaks()
+    out = {"workload": f"blast wave 3-D {a.n}^3 interior, periodic, RK4, hyperdiffusion on, single simulation",
+           "cells_with_ghosts": prob.ncells}
+    for name, prec, bpc in (("mixed", PREC_MIXED, BYTES_PER_CELL_UPDATE_MIXED_3D),
+                            ("fp64", PREC_FP64, BYTES_PER_CELL_UPDATE_FP64_3D)):
+        eng = Engine(prob, rk4=True, device=ctx.local, precision=prec)
+        m = measure(eng, n_int, a.steps, a.warmup, ctx, sample_clocks=False)
+        alg = bpc / 4 * n_int
+        ach = alg / (m["avg_stage_ms"] / 1e3) / 1e9
+        out[name] = {"value": m["value"], "ms_per_step": m["ms_per_step"], "avg_stage_ms": m["avg_stage_ms"],
+                     "roofline": {"achieved": ach, "peak": peak, "frac": ach / peak, "unit": "GB/s",
+                                  "alg_bytes_per_launch": alg}}
+        if name == "mixed":
+            # every step: smaug_set_state from pinned host memory, smaug_step,
+            # smaug_get_state and smaug_get_scalars back to the host
+            dptr = ctypes.POINTER(ctypes.c_double)
+            host = torch.from_numpy(np.ascontiguousarray(prob.w)).pin_memory()
+            hp = host.numpy().ctypes.data_as(dptr)
+            scal = (ctypes.c_double * 8)()
 
-    # ---- headline: K steps, device time on the engine's stream
-    m = measure(eng, n_int, a.steps, a.warmup, stream, barrier, dist, world, local, sample_clocks=True)
-    alg_bytes_per_launch = (BYTES_PER_CELL_UPDATE_MIXED_3D if mixed else BYTES_PER_CELL_UPDATE_FP64_3D) / 4 * n_int
-    achieved = alg_bytes_per_launch / (m["avg_stage_ms"] / 1e3) / 1e9
+            def loop():
+                for _ in range(a.steps):
+                    eng.lib.smaug_set_state(eng.h, hp, host.numel())
+                    eng.lib.smaug_step(eng.h, 1)
+                    eng.lib.smaug_get_state(eng.h, hp, host.numel())
+                    eng.lib.smaug_get_scalars(eng.h, scal)
+
+            ctx.barrier()
+            torch.cuda.synchronize()
+            ms = ctx.max_ms(event_ms(torch.cuda.ExternalStream(eng.stream), loop))
+            out["mixed"]["e2e_per_step_round_trip"] = {
+                "value": ctx.world * n_int * a.steps / (ms / 1e3), "h2d_bytes_per_step": host.numel() * 8,
+                "d2h_bytes_per_step": host.numel() * 8 + 64}
+        eng.close()
+    out["mixed_vs_fp64"] = out["mixed"]["value"] / out["fp64"]["value"]
+    if a.accuracy_steps > 0 and ctx.rank == 0:
+        out["accuracy"] = accuracy_study(prob, a.accuracy_steps, ctx.local)
+    return out
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--n", type=int, default=128, help="blast wave: interior cells per dim")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-plain", action="store_true", help="skip the plain FP64 single-simulation ensemble run")
+    ap.add_argument("--no-blast", action="store_true", help="skip the 3-D blast wave measurements")
+    ap.add_argument("--only-batched", action="store_true", help="just the timed batched run (profiling)")
+    ap.add_argument("--ensemble-count", type=int, default=ENSEMBLE["count"])
+    ap.add_argument("--accuracy-steps", type=int, default=50,
+                    help="steps of the blast-wave accuracy study against the FP64 oracle build (0: skip)")
+    a = ap.parse_args()
+    if a.impl == "reference":
+        return run_reference(a)
+
+    from smaug_b200 import PREC_FP64, PREC_MIXED, problems
+    ctx = Ctx(a)
+    W, K = max(3, a.warmup), a.steps
+    probs = problems.ensemble(a.ensemble_count, seed=ENSEMBLE["seed"] + 1000 * ctx.rank)
+    cells = sum(p.interior for p in probs)
+
+    head = run_batched(probs, PREC_MIXED, ctx, K, W, sample_clocks=True)
+    line_extra = {}
+    if not a.only_batched:
+        line_extra["batched_fp64"] = {k: v for k, v in run_batched(probs, PREC_FP64, ctx, K, W, False).items()
+                                      if k in ("value", "ms_per_step", "avg_stage_ms", "tile_variant")}
+        if not a.no_plain:
+            plain = run_plain(probs, PREC_FP64, ctx, K, W)
+            line_extra["plain_fp64"] = dict(plain, path="single-simulation context, FP64, one simulation after "
+                                                        "another (smaug_create / smaug_step)")
+            line_extra["batched_vs_plain_fp64"] = head["value"] / plain["value"]
+        e2e = run_e2e_batched(probs, PREC_MIXED, ctx, K)
+        if not a.no_blast:
+            line_extra["blast128"] = run_blast(a, ctx)
+    else:
+        e2e = None
+
+    alg = BYTES_PER_CELL_UPDATE_MIXED_2D / 4 * cells
+    achieved = alg / (head["avg_stage_ms"] / 1e3) / 1e9
     peak, peak_kind = load_peaks()
     tr = load_traffic()
-    traffic = None
-    kernel = f"tile_stage_kernel<3,{'float' if mixed else 'double'}>"
-    if tr and tr.get(kernel, {}).get("n") == a.n:
-        traffic = tr[kernel].get("dram_bytes_per_launch")
-
-    # ---- the other precision on the same workload
-    companion = None
-    if not a.no_companion:
-        eng2 = Engine(prob, rk4=True, exact=False, device=local, precision=PREC_FP64 if mixed else PREC_MIXED)
-        s2 = torch.cuda.ExternalStream(eng2.stream)
-        m2 = measure(eng2, n_int, a.steps, a.warmup, s2, barrier, dist, world, local, sample_clocks=False)
-        companion = {"precision": "fp64" if mixed else "mixed", "value": m2["value"],
-                     "ms_per_step": m2["ms_per_step"], "avg_stage_ms": m2["avg_stage_ms"]}
-        eng2.close()
-
-    # ---- accuracy against the FP64 oracle (the FMA-free FP64 build, which
-    # reproduces it bit for bit), beside the drift of the FP64 FMA build
-    accuracy = None
-    if a.accuracy_steps > 0 and rank == 0:
-        accuracy = accuracy_study(prob, a.accuracy_steps, local)
-
-    # ---- end to end through the public C ABI with host buffers: every step
-    # uploads its input state from pinned host memory (smaug_set_state),
-    # advances one step (smaug_step) and reads the new state and the step's
-    # scalars back (smaug_get_state, smaug_get_scalars)
-    dptr = ctypes.POINTER(ctypes.c_double)
-    host = torch.from_numpy(np.ascontiguousarray(prob.w)).pin_memory()
-    host_p = host.numpy().ctypes.data_as(dptr)
-    scal = (ctypes.c_double * 8)()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    barrier()
-    torch.cuda.synchronize()
-    e0.record(stream)
-    for _ in range(a.steps):
-        eng.lib.smaug_set_state(eng.h, host_p, host.numel())
-        eng.lib.smaug_step(eng.h, 1)
-        eng.lib.smaug_get_state(eng.h, host_p, host.numel())
-        eng.lib.smaug_get_scalars(eng.h, scal)
-    e1.record(stream)
-    torch.cuda.synchronize()
-    e2e_ms = e0.elapsed_time(e1)
-    te = torch.tensor([e2e_ms], device="cuda")
-    if dist is not None:
-        dist.all_reduce(te, op=dist.ReduceOp.MAX)
-    e2e_value = world * n_int * a.steps / (float(te.item()) / 1e3)
-    state_bytes = host.numel() * 8
+    kernel = "batch_stage_kernel<2,float>"
+    traffic = tr.get(kernel, {}).get("dram_bytes_per_launch") if tr else None
 
     cpu = None
-    if rank == 0 and world == 1 and not a.no_cpu_baseline:
+    if ctx.rank == 0 and ctx.world == 1 and not a.no_cpu_baseline and not a.only_batched:
         try:
             cpu = cpu_throughput(nsteps=2, warmup=1)
             cpu = {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")}
         except Exception as ex:  # the GPU number stands on its own
             cpu = {"value": None, "unit": UNIT, "cores": 0, "kind": "reference", "sample": f"failed: {ex}"}
 
-    if rank == 0:
-        cfg = workload_config(a.n, world, prob.ncells)
-        cfg["precision"] = "mixed: FP32 states/stencils, FP64 p_T, e_int, base, RK sum, dt" if mixed else "fp64"
+    if ctx.rank == 0:
+        cfg = workload_config(ctx.world, cells)
+        cfg["precision"] = "mixed: FP32 stage states/stencils; FP64 backgrounds, p_T, e_int, RK base + sum, dt"
+        cfg["tile_variant"] = head["tile_variant"]
         line = {
-            "metric": METRIC, "value": m["value"], "unit": UNIT, "n_gpus": world, "steps": a.steps,
-            "warmup": max(3, a.warmup), "ms_per_step": m["ms_per_step"], "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64" if mixed else "f64", "data": "synthetic",
-            "config": cfg,
+            "metric": METRIC, "value": head["value"], "unit": UNIT, "n_gpus": ctx.world, "steps": K,
+            "warmup": W, "ms_per_step": head["ms_per_step"], "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic", "config": cfg,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic, "peak_source": peak_kind,
-                         "kernel": kernel, "avg_launch_ms": m["avg_stage_ms"],
-                         "alg_bytes_per_launch": alg_bytes_per_launch},
+                         "kernel": kernel, "avg_launch_ms": head["avg_stage_ms"], "alg_bytes_per_launch": alg},
             "cpu_baseline": cpu,
-            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": state_bytes,
-                    "d2h_bytes_per_step": state_bytes + 8 * 8},
-            "gpu_launches": m["launches"],
-            "clocks": m["clocks"],
+            "e2e": e2e,
+            "gpu_launches": head["launches"],
+            "clocks": head["clocks"],
         }
-        if companion:
-            line["companion"] = companion
-            line["mixed_vs_fp64"] = (m["value"] / companion["value"]) if mixed else (companion["value"] / m["value"])
-        if accuracy:
-            line["accuracy"] = accuracy
+        line.update(line_extra)
         print(json.dumps(line))
-    eng.close()
-    if dist is not None:
-        dist.barrier()
-        dist.destroy_process_group()
+    if ctx.dist is not None:
+        ctx.barrier()
+        ctx.dist.destroy_process_group()
     return 0
 
 

@@ -48,7 +48,8 @@ enum {
   SMAUG_ERR_ARG = -1,      /* invalid argument or size */
   SMAUG_ERR_CUDA = -2,     /* CUDA runtime error */
   SMAUG_ERR_STATE = -3,    /* call out of order (e.g. step before set_state) */
-  SMAUG_ERR_NONFINITE = -4 /* dt or a reduction became NaN/Inf */
+  SMAUG_ERR_NONFINITE = -4, /* dt or a reduction became NaN/Inf */
+  SMAUG_ERR_FULL = -5       /* batch: no free slot or arena block for a simulation */
 };
 
 /* Boundary types per direction (iotypes.h:145 boundtype codes). */
@@ -81,6 +82,25 @@ typedef struct {
   double dt0;       /* initial dt (1e-8 when dt_mode = 1, iosmaug.cpp:327-330) */
   int exact;        /* 1: kernels built without FMA contraction (bit-reproducible) */
   int precision;    /* SMAUG_PREC_FP64 (default, 0) or SMAUG_PREC_MIXED */
+  /*
+   * Momentum driver (the reference's user source term, addsourceterms2 of
+   * models/usersource.cu.spicule1:4-137, applied by cusource at
+   * iosmaug.cpp:1153): after each stage's update, at every cell,
+   *   m_dir += h * (drv_amp * F(x) * tdep(t)) * (rho + rhob)
+   * with F the product over dims of exp(-(x_d - drv_center[d])^2 /
+   * drv_width[d]^2) (1 along a dim whose width is 0), x_d = xmin[d] + i_d *
+   * dx[d] (the reference's p->xmin, p->dx), and tdep = sin(2 pi t /
+   * drv_period), or 1 when drv_period = 0 (the reference model's choice).
+   * t is the stage's input time.  drv_on = 0 switches it off.
+   */
+  int drv_on;
+  int drv_dir;            /* driven momentum component, 0 .. ndim-1 */
+  double drv_amp;
+  double drv_period;
+  double drv_center[3];
+  double drv_width[3];
+  double xmin[3];         /* coordinate of cell 0 (a ghost) per dim */
+  double dx[3];           /* grid spacing per dim */
 } smaug_params;
 
 /* Number of fields for ndim (10 or 13). */
@@ -142,7 +162,8 @@ int smaug_stage_times(smaug_ctx *ctx, double *ms_total, long long *count);
  * Runge-Kutta stage buffers and the device-side scalars live in a file-scope
  * device array of SMAUG_NOALLOC_SCRATCH_BYTES that every GPU which loads the
  * library holds until the process exits.  Grids whose scratch would not fit
- * (3 * (2 + 2*ndim) * N doubles plus the metric lines and the scalars) are
+ * (3 * (2 + 2*ndim) * N doubles plus the metric lines, the scalars and a
+ * 1-simulation descriptor for the stage kernel) are
  * rejected with SMAUG_ERR_ARG and a message in err.
  *
  * Each call starts afresh from w_in (dt from dt0 / the reference's dt rule,
@@ -158,6 +179,71 @@ int smaug_stage_times(smaug_ctx *ctx, double *ms_total, long long *count);
 int smaug_step_noalloc(const smaug_params *prm, const double *delx_dev, const double *w_in_dev,
                        double *w_out_dev, int nsteps, void *stream, double *scalars_out, char *err,
                        size_t errlen);
+
+/*
+ * Batches -- no counterpart in the reference (one SMAUG process runs one
+ * simulation).  A batch holds many independent simulations of one ndim and
+ * one precision, each of its own size and parameters, in one device arena
+ * allocated at creation.  smaug_batch_step advances every simulation that
+ * still has steps left by one RK4 step per step: one launch per RK stage for
+ * all of them (a persistent kernel over a (simulation, tile) work list),
+ * replayed from CUDA graphs.  Each simulation keeps its own dt (the
+ * reference's rule, or fixed), maxima and status; its results are the same
+ * as those of a context with the same smaug_params (the same kernel
+ * arithmetic).  Simulations are added and removed between calls, on the
+ * batch's stream; a finished simulation stops taking steps on the device.
+ * All simulations use rk4 = 1 and exact = 0.
+ */
+typedef struct smaug_batch smaug_batch;
+
+/* Arena bytes one simulation of these parameters takes (host only). */
+int smaug_batch_footprint(const smaug_params *prm, size_t *bytes);
+
+int smaug_batch_create(int ndim, int precision, int device, size_t arena_bytes, int max_sims,
+                       smaug_batch **out);
+int smaug_batch_destroy(smaug_batch *b);
+
+/*
+ * Admit a simulation: prm as for smaug_create (ndim and precision those of
+ * the batch), delx as for smaug_set_metric, w as for smaug_set_state (host
+ * buffers, copied before the call returns), nsteps = RK4 steps to take.
+ * Returns SMAUG_ERR_FULL when no slot or no arena block is free.
+ */
+int smaug_batch_add(smaug_batch *b, const smaug_params *prm, const double *delx, const double *w,
+                    long long nsteps, int *slot);
+int smaug_batch_remove(smaug_batch *b, int slot);
+
+/* Enqueue nsteps batch steps (asynchronous). */
+int smaug_batch_step(smaug_batch *b, int nsteps);
+
+/* Steps left per slot (n >= max_sims entries; -1 for a free slot).  Waits. */
+int smaug_batch_poll(smaug_batch *b, long long *steps_left, int n);
+
+/* Wait; returns the first simulation error (its slot in *bad_slot, may be NULL). */
+int smaug_batch_sync(smaug_batch *b, int *bad_slot);
+
+/* One simulation's state (NVAR * N doubles) and scalars (as smaug_get_scalars). */
+int smaug_batch_get_state(smaug_batch *b, int slot, double *w, size_t count);
+int smaug_batch_get_scalars(smaug_batch *b, int slot, double out[8]);
+
+/*
+ * Autotuner: times RK stage 1 of the current simulations with every tile
+ * shape the stage kernel is built for (reps launches each) and keeps the
+ * fastest.  ms_out (nms entries, may be NULL) receives the per-shape times.
+ */
+int smaug_batch_tune(smaug_batch *b, int reps, int *variant_out, double *ms_out, int nms);
+int smaug_batch_set_variant(smaug_batch *b, int variant);
+
+/* Stage timing, as smaug_profile_stages / smaug_stage_times (while it is on,
+ * steps are launched directly instead of from CUDA graphs). */
+int smaug_batch_profile_stages(smaug_batch *b, int enable);
+int smaug_batch_stage_times(smaug_batch *b, double *ms_total, long long *count);
+
+/* Free arena bytes, the largest free block, simulations held. */
+int smaug_batch_info(smaug_batch *b, size_t *free_bytes, size_t *largest_free, int *sims);
+void *smaug_batch_stream(smaug_batch *b);
+long long smaug_batch_launch_count(smaug_batch *b);
+const char *smaug_batch_last_error(smaug_batch *b);
 
 /* The CUDA stream (cudaStream_t) all work of ctx is ordered on. */
 void *smaug_stream(smaug_ctx *ctx);

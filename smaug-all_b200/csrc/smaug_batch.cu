@@ -1,0 +1,597 @@
+// smaug_batch.cu -- host side of the batch C ABI (smaug_batch_* in
+// include/smaug_b200.h).
+//
+// A batch holds many independent simulations of one ndim and one precision,
+// of any sizes, in one device arena.  A batch step is six launches for all
+// of them together:
+//   batch_dt_kernel        per simulation: the reference's dt rule, and
+//                          whether it takes this step (steps left, status)
+//   batch stage kernel x4  one persistent launch per RK stage over the work
+//                          list of (simulation, tile) items
+//   batch_finish_kernel    per simulation: running maxima, status
+// and a chunk of steps is replayed from a CUDA graph.  Simulations are added
+// and removed between steps (admission by arena footprint); finished ones
+// stop taking steps on the device without a host round trip.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+#include <map>
+#include <string>
+#include <vector>
+
+#include "../../include/smaug_b200.h"
+#include "smaug_batch.cuh"
+#include "smaug_common.cuh"
+
+namespace {
+
+constexpr int kGraphSteps = 16;  // steps per replay of the long graph
+
+__global__ void batch_dt_kernel(BatchInst *tab, long long *left, int *status, int n, int D) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  BatchInst &I = tab[i];
+  if (!I.active) return;
+  DevScalars *sc = I.sc;
+  if (left[i] > 0 && sc->status == 0) {
+    dt_update(sc, I.phys, D);
+    sc->go = 1;
+    left[i] -= 1;
+  } else {
+    sc->go = 0;
+  }
+  status[i] = sc->status;
+}
+
+__global__ void batch_finish_kernel(BatchInst *tab, int *status, int n) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  BatchInst &I = tab[i];
+  if (!I.active || !I.sc->go) return;
+  finish_update(I.sc, 4);
+  status[i] = I.sc->status;
+}
+
+// Every simulation in the batch takes stage 1 (autotuning only: stage 1
+// writes scratch buffers that the next real step rewrites).
+__global__ void batch_go_kernel(BatchInst *tab, int n) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n && tab[i].active) tab[i].sc->go = 1;
+}
+
+__global__ void one_reset_kernel(DevScalars *sc, double dt0) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) reset_update(sc, dt0);
+}
+
+size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
+
+// Arena bytes one simulation takes (the order below is the carve order).
+size_t sim_footprint(const SimPlan &p) {
+  const size_t N = (size_t)p.geo.N;
+  size_t b = align256(sizeof(DevScalars));
+  b += 2 * align256(sizeof(double) * (size_t)(p.geo.n[0] + p.geo.n[1] + p.geo.n[2]));  // metric, driver
+  b += align256(sizeof(double) * N);                  // dxlast
+  b += align256(sizeof(double) * (size_t)p.NB * N);   // backgrounds
+  b += align256(sizeof(double) * (size_t)p.NW * N);   // W[0]
+  if (p.mixed)
+    b += 5 * align256(sizeof(float) * (size_t)p.NW * N);
+  else
+    b += 3 * align256(sizeof(double) * (size_t)p.NW * N);
+  return b;
+}
+
+struct Slot {
+  bool used = false;
+  size_t off = 0, bytes = 0;
+  SimPlan plan;
+  long long steps_total = 0;
+};
+
+}  // namespace
+
+struct smaug_batch {
+  int D = 0, device = 0;
+  bool mixed = false;
+  int max_inst = 0;
+  cudaStream_t stream = nullptr, cap = nullptr;
+  char *arena = nullptr;
+  size_t arena_bytes = 0;
+  std::map<size_t, size_t> free_;  // offset -> size
+  BatchInst *d_tab = nullptr;
+  long long *d_left = nullptr;
+  int *d_status = nullptr;
+  std::vector<BatchInst> h_tab;
+  std::vector<Slot> slots;
+  WorkItem *d_work = nullptr;
+  size_t work_cap = 0;
+  int nwork = 0, grid = 0, variant = 0, sms = 148;
+  bool dirty = true;
+  cudaGraphExec_t g1 = nullptr, gk = nullptr;
+  long long launches = 0;
+  // stage timing: steps are then launched directly, each stage kernel
+  // bracketed by events
+  bool profile = false;
+  std::vector<cudaEvent_t> ev;
+  size_t ev_used = 0;
+  std::string err;
+};
+
+namespace {
+
+int bfail(smaug_batch *b, int code, const std::string &m) {
+  if (b) b->err = m;
+  return code;
+}
+
+#define BK(call)                                                                                         \
+  do {                                                                                                   \
+    cudaError_t e_ = (call);                                                                             \
+    if (e_ != cudaSuccess) return bfail(b, SMAUG_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+  } while (0)
+
+bool arena_alloc(smaug_batch *b, size_t bytes, size_t *off) {
+  for (auto it = b->free_.begin(); it != b->free_.end(); ++it) {
+    if (it->second >= bytes) {
+      *off = it->first;
+      const size_t rest = it->second - bytes, o = it->first + bytes;
+      b->free_.erase(it);
+      if (rest) b->free_[o] = rest;
+      return true;
+    }
+  }
+  return false;
+}
+
+void arena_free(smaug_batch *b, size_t off, size_t bytes) {
+  auto it = b->free_.emplace(off, bytes).first;
+  auto nx = std::next(it);
+  if (nx != b->free_.end() && it->first + it->second == nx->first) {
+    it->second += nx->second;
+    b->free_.erase(nx);
+  }
+  if (it != b->free_.begin()) {
+    auto pv = std::prev(it);
+    if (pv->first + pv->second == it->first) {
+      pv->second += it->second;
+      b->free_.erase(it);
+    }
+  }
+}
+
+void drop_graphs(smaug_batch *b) {
+  if (b->g1) cudaGraphExecDestroy(b->g1);
+  if (b->gk) cudaGraphExecDestroy(b->gk);
+  b->g1 = b->gk = nullptr;
+}
+
+// Tiles per dim of a simulation for the batch's tile shape.
+void set_tiles(const smaug_batch *b, BatchInst &I) {
+  int t[3];
+  batch_tile_shape(b->D, b->variant, t);
+  for (int d = 0; d < 3; ++d) I.tiles[d] = d < b->D ? (I.geo.n[d] - 4 + t[d] - 1) / t[d] : 1;
+}
+
+// Rebuild the work list and the persistent grid for the current simulations
+// and tile shape.
+int rebuild(smaug_batch *b) {
+  std::vector<WorkItem> w;
+  for (int i = 0; i < b->max_inst; ++i) {
+    if (!b->slots[i].used) continue;
+    set_tiles(b, b->h_tab[i]);
+    const int nt = b->h_tab[i].tiles[0] * b->h_tab[i].tiles[1] * b->h_tab[i].tiles[2];
+    for (int t = 0; t < nt; ++t) w.push_back({i, t});
+  }
+  BK(cudaMemcpyAsync(b->d_tab, b->h_tab.data(), sizeof(BatchInst) * b->max_inst, cudaMemcpyHostToDevice, b->stream));
+  if (w.size() > b->work_cap) {
+    BK(cudaStreamSynchronize(b->stream));
+    if (b->d_work) cudaFree(b->d_work);
+    b->work_cap = std::max(w.size(), (size_t)1024) * 2;
+    BK(cudaMalloc(&b->d_work, sizeof(WorkItem) * b->work_cap));
+  }
+  if (!w.empty())
+    BK(cudaMemcpyAsync(b->d_work, w.data(), sizeof(WorkItem) * w.size(), cudaMemcpyHostToDevice, b->stream));
+  // the copy source is pageable host memory: wait for it before w goes away
+  BK(cudaStreamSynchronize(b->stream));
+  b->nwork = (int)w.size();
+  const int occ = std::max(1, smaug_batchk::batch_stage_occupancy(b->D, b->mixed, b->variant));
+  b->grid = std::min(b->nwork, occ * b->sms);
+  drop_graphs(b);
+  b->dirty = false;
+  return SMAUG_OK;
+}
+
+void enqueue_step(smaug_batch *b, cudaStream_t s, bool timed = false) {
+  const int nb = (b->max_inst + 127) / 128;
+  batch_dt_kernel<<<nb, 128, 0, s>>>(b->d_tab, b->d_left, b->d_status, b->max_inst, b->D);
+  for (int k = 1; k <= 4; ++k) {
+    cudaEvent_t e1 = nullptr;
+    if (timed) {
+      while (b->ev.size() < b->ev_used + 2) {
+        cudaEvent_t e;
+        if (cudaEventCreate(&e) != cudaSuccess) break;
+        b->ev.push_back(e);
+      }
+      if (b->ev.size() >= b->ev_used + 2) {
+        cudaEventRecord(b->ev[b->ev_used], s);
+        e1 = b->ev[b->ev_used + 1];
+        b->ev_used += 2;
+      }
+    }
+    smaug_batchk::launch_batch_stage(b->D, b->mixed, b->variant, b->d_tab, b->d_work, b->nwork, k, b->grid, s);
+    if (e1) cudaEventRecord(e1, s);
+  }
+  batch_finish_kernel<<<nb, 128, 0, s>>>(b->d_tab, b->d_status, b->max_inst);
+}
+
+int capture(smaug_batch *b, int steps, cudaGraphExec_t *out) {
+  cudaGraph_t g = nullptr;
+  BK(cudaStreamBeginCapture(b->cap, cudaStreamCaptureModeThreadLocal));
+  for (int i = 0; i < steps; ++i) enqueue_step(b, b->cap);
+  BK(cudaStreamEndCapture(b->cap, &g));
+  cudaError_t e = cudaGraphInstantiate(out, g, 0);
+  cudaGraphDestroy(g);
+  BK(e);
+  return SMAUG_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int smaug_batch_footprint(const smaug_params *prm, size_t *bytes) {
+  if (!prm || !bytes) return SMAUG_ERR_ARG;
+  SimPlan p;
+  if (plan_sim(prm, p)) return SMAUG_ERR_ARG;
+  *bytes = sim_footprint(p);
+  return SMAUG_OK;
+}
+
+int smaug_batch_create(int ndim, int precision, int device, size_t arena_bytes, int max_sims, smaug_batch **out) {
+  if (!out) return SMAUG_ERR_ARG;
+  *out = nullptr;
+  smaug_batch *b = new smaug_batch();
+  *out = b;
+  if (ndim != 2 && ndim != 3) return bfail(b, SMAUG_ERR_ARG, "ndim must be 2 or 3");
+  if (precision != SMAUG_PREC_FP64 && precision != SMAUG_PREC_MIXED)
+    return bfail(b, SMAUG_ERR_ARG, "precision must be SMAUG_PREC_FP64 or SMAUG_PREC_MIXED");
+  if (max_sims < 1 || max_sims > (1 << 16)) return bfail(b, SMAUG_ERR_ARG, "max_sims must be 1..65536");
+  if (arena_bytes < 4096) return bfail(b, SMAUG_ERR_ARG, "arena too small");
+  b->D = ndim;
+  b->mixed = precision == SMAUG_PREC_MIXED;
+  b->device = device;
+  b->max_inst = max_sims;
+  b->arena_bytes = arena_bytes & ~(size_t)255;
+  b->h_tab.assign(max_sims, BatchInst{});
+  b->slots.assign(max_sims, Slot{});
+  BK(cudaSetDevice(device));
+  int sms = 0;
+  BK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+  b->sms = sms > 0 ? sms : 148;
+  BK(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking));
+  BK(cudaStreamCreateWithFlags(&b->cap, cudaStreamNonBlocking));
+  BK(cudaMalloc(&b->arena, b->arena_bytes));
+  b->free_[0] = b->arena_bytes;
+  BK(cudaMalloc(&b->d_tab, sizeof(BatchInst) * max_sims));
+  BK(cudaMalloc(&b->d_left, sizeof(long long) * max_sims));
+  BK(cudaMalloc(&b->d_status, sizeof(int) * max_sims));
+  BK(cudaMemsetAsync(b->d_tab, 0, sizeof(BatchInst) * max_sims, b->stream));
+  BK(cudaMemsetAsync(b->d_left, 0, sizeof(long long) * max_sims, b->stream));
+  BK(cudaMemsetAsync(b->d_status, 0, sizeof(int) * max_sims, b->stream));
+  BK(cudaStreamSynchronize(b->stream));
+  return SMAUG_OK;
+}
+
+int smaug_batch_destroy(smaug_batch *b) {
+  if (!b) return SMAUG_OK;
+  cudaSetDevice(b->device);
+  if (b->stream) cudaStreamSynchronize(b->stream);
+  drop_graphs(b);
+  for (auto e : b->ev) cudaEventDestroy(e);
+  cudaFree(b->arena);
+  cudaFree(b->d_tab);
+  cudaFree(b->d_left);
+  cudaFree(b->d_status);
+  cudaFree(b->d_work);
+  if (b->stream) cudaStreamDestroy(b->stream);
+  if (b->cap) cudaStreamDestroy(b->cap);
+  delete b;
+  return SMAUG_OK;
+}
+
+int smaug_batch_add(smaug_batch *b, const smaug_params *prm, const double *delx, const double *w, long long nsteps,
+                    int *slot_out) {
+  if (!b || !prm || !delx || !w || !slot_out || nsteps < 0) return SMAUG_ERR_ARG;
+  *slot_out = -1;
+  SimPlan p;
+  if (const char *m = plan_sim(prm, p)) return bfail(b, SMAUG_ERR_ARG, m);
+  if (p.D != b->D) return bfail(b, SMAUG_ERR_ARG, "simulation ndim differs from the batch's");
+  if (p.mixed != b->mixed) return bfail(b, SMAUG_ERR_ARG, "simulation precision differs from the batch's");
+  if (!p.rk4 || p.exact) return bfail(b, SMAUG_ERR_ARG, "batch simulations use rk4 = 1 and exact = 0");
+  const long long N = p.geo.N;
+  std::vector<double> d1(p.geo.n[0] + p.geo.n[1] + p.geo.n[2]);
+  double minsq[3];
+  if (const char *m = metric_host(p, delx, d1.data(), minsq)) return bfail(b, SMAUG_ERR_ARG, m);
+  int slot = -1;
+  for (int i = 0; i < b->max_inst; ++i)
+    if (!b->slots[i].used) {
+      slot = i;
+      break;
+    }
+  if (slot < 0) return bfail(b, SMAUG_ERR_FULL, "no free simulation slot");
+  const size_t fp = sim_footprint(p);
+  size_t off = 0;
+  if (!arena_alloc(b, fp, &off)) return bfail(b, SMAUG_ERR_FULL, "arena has no free block of the simulation's footprint");
+  BK(cudaSetDevice(b->device));
+  // carve
+  char *q = b->arena + off;
+  auto take = [&](size_t bytes) {
+    char *r = q;
+    q += align256(bytes);
+    return r;
+  };
+  DevScalars *sc = (DevScalars *)take(sizeof(DevScalars));
+  double *dx1 = (double *)take(sizeof(double) * d1.size());
+  double *drv = (double *)take(sizeof(double) * d1.size());
+  std::vector<double> drv_host(d1.size());
+  driver_lines(p, prm, drv_host.data());
+  double *dxlast = (double *)take(sizeof(double) * N);
+  double *bg = (double *)take(sizeof(double) * p.NB * N);
+  BatchInst I{};
+  I.W[0] = (double *)take(sizeof(double) * p.NW * N);
+  if (p.mixed)
+    for (auto &f : I.F) f = (float *)take(sizeof(float) * p.NW * N);
+  else
+    for (int k = 1; k < 4; ++k) I.W[k] = (double *)take(sizeof(double) * p.NW * N);
+  // backgrounds: are the energy background terms live?
+  int has = 0;
+  const double *bh = w + (size_t)N * p.NW;
+  for (long long j = 0; j < N && !has; ++j) {
+    if (bh[j] != 0.0) has = 1;
+    for (int k = 0; k < p.D; ++k)
+      if (bh[(size_t)(2 + k) * N + j] != 0.0) has = 1;
+  }
+  p.phys.has_bgb = has;
+  size_t o1 = 0;
+  for (int d = 0; d < p.D; ++d) {
+    p.geo.dx1[d] = dx1 + o1;
+    o1 += p.geo.n[d];
+  }
+  p.geo.dxlast = dxlast;
+  o1 = 0;
+  for (int d = 0; d < 3; ++d) {
+    p.geo.drvf[d] = drv + o1;
+    o1 += p.geo.n[d];
+  }
+  I.geo = p.geo;
+  I.phys = p.phys;
+  I.bg = bg;
+  I.sc = sc;
+  I.active = 1;
+  cudaStream_t s = b->stream;
+  BK(cudaMemsetAsync(sc, 0, sizeof(DevScalars), s));
+  BK(cudaMemcpyAsync(sc->minsq, minsq, sizeof(minsq), cudaMemcpyHostToDevice, s));
+  BK(cudaMemcpyAsync(dx1, d1.data(), sizeof(double) * d1.size(), cudaMemcpyHostToDevice, s));
+  BK(cudaMemcpyAsync(drv, drv_host.data(), sizeof(double) * drv_host.size(), cudaMemcpyHostToDevice, s));
+  BK(cudaMemcpyAsync(dxlast, delx + (size_t)(p.D - 1) * N, sizeof(double) * N, cudaMemcpyHostToDevice, s));
+  BK(cudaMemcpyAsync(I.W[0], w, sizeof(double) * p.NW * N, cudaMemcpyHostToDevice, s));
+  BK(cudaMemcpyAsync(bg, bh, sizeof(double) * p.NB * N, cudaMemcpyHostToDevice, s));
+  ghost_fill_kernel<<<148 * 8, 256, 0, s>>>(I.W[0], p.NW, p.geo, p.D);
+  const double dt0 = p.phys.dt_mode == 1 ? (p.dt0 > 0 ? p.dt0 : 1.0e-8) : p.dt0;
+  one_reset_kernel<<<1, 1, 0, s>>>(sc, dt0);
+  smaug_fast::launch_reduce(p.D, I.W[0], bg, p.geo, p.phys, &sc->red[0], s);
+  if (p.mixed) split_kernel<<<148 * 8, 256, 0, s>>>(I.W[0], I.F[0], I.F[1], (long long)p.NW * N);
+  b->launches += p.mixed ? 4 : 3;
+  BK(cudaGetLastError());
+  BK(cudaMemcpyAsync(b->d_left + slot, &nsteps, sizeof(long long), cudaMemcpyHostToDevice, s));
+  const int zero = 0;
+  BK(cudaMemcpyAsync(b->d_status + slot, &zero, sizeof(int), cudaMemcpyHostToDevice, s));
+  BK(cudaStreamSynchronize(s));  // the sources above are host temporaries
+  Slot &S = b->slots[slot];
+  S.used = true;
+  S.off = off;
+  S.bytes = fp;
+  S.plan = p;
+  S.steps_total = nsteps;
+  b->h_tab[slot] = I;
+  b->dirty = true;
+  *slot_out = slot;
+  return SMAUG_OK;
+}
+
+int smaug_batch_remove(smaug_batch *b, int slot) {
+  if (!b || slot < 0 || slot >= b->max_inst || !b->slots[slot].used) return SMAUG_ERR_ARG;
+  BK(cudaSetDevice(b->device));
+  // queued steps may still use the slot's memory: stream order keeps a later
+  // simulation's uploads behind them
+  b->h_tab[slot] = BatchInst{};
+  arena_free(b, b->slots[slot].off, b->slots[slot].bytes);
+  b->slots[slot] = Slot{};
+  b->dirty = true;
+  return SMAUG_OK;
+}
+
+int smaug_batch_step(smaug_batch *b, int nsteps) {
+  if (!b || nsteps < 0) return SMAUG_ERR_ARG;
+  BK(cudaSetDevice(b->device));
+  if (b->dirty) {
+    int rc = rebuild(b);
+    if (rc != SMAUG_OK) return rc;
+  }
+  if (b->nwork == 0) return SMAUG_OK;
+  if (b->profile) {
+    for (int i = 0; i < nsteps; ++i) enqueue_step(b, b->stream, true);
+    b->launches += 6LL * nsteps;
+    BK(cudaGetLastError());
+    return SMAUG_OK;
+  }
+  if (nsteps >= kGraphSteps && !b->gk) {
+    int rc = capture(b, kGraphSteps, &b->gk);
+    if (rc != SMAUG_OK) return rc;
+  }
+  if (nsteps % kGraphSteps && !b->g1) {
+    int rc = capture(b, 1, &b->g1);
+    if (rc != SMAUG_OK) return rc;
+  }
+  for (int i = 0; i + kGraphSteps <= nsteps; i += kGraphSteps) {
+    BK(cudaGraphLaunch(b->gk, b->stream));
+    b->launches += 6LL * kGraphSteps;
+  }
+  for (int i = 0; i < nsteps % kGraphSteps; ++i) {
+    BK(cudaGraphLaunch(b->g1, b->stream));
+    b->launches += 6;
+  }
+  return SMAUG_OK;
+}
+
+int smaug_batch_poll(smaug_batch *b, long long *steps_left, int n) {
+  if (!b || !steps_left || n < b->max_inst) return SMAUG_ERR_ARG;
+  BK(cudaSetDevice(b->device));
+  BK(cudaMemcpyAsync(steps_left, b->d_left, sizeof(long long) * b->max_inst, cudaMemcpyDeviceToHost, b->stream));
+  BK(cudaStreamSynchronize(b->stream));
+  for (int i = 0; i < b->max_inst; ++i)
+    if (!b->slots[i].used) steps_left[i] = -1;
+  return SMAUG_OK;
+}
+
+int smaug_batch_sync(smaug_batch *b, int *bad_slot) {
+  if (!b) return SMAUG_ERR_ARG;
+  if (bad_slot) *bad_slot = -1;
+  BK(cudaSetDevice(b->device));
+  std::vector<int> st(b->max_inst);
+  BK(cudaMemcpyAsync(st.data(), b->d_status, sizeof(int) * b->max_inst, cudaMemcpyDeviceToHost, b->stream));
+  BK(cudaStreamSynchronize(b->stream));
+  for (int i = 0; i < b->max_inst; ++i)
+    if (b->slots[i].used && st[i] != 0) {
+      if (bad_slot) *bad_slot = i;
+      return bfail(b, st[i], "simulation " + std::to_string(i) + ": non-finite dt or wave speed");
+    }
+  return SMAUG_OK;
+}
+
+int smaug_batch_get_state(smaug_batch *b, int slot, double *w, size_t count) {
+  if (!b || !w || slot < 0 || slot >= b->max_inst || !b->slots[slot].used) return SMAUG_ERR_ARG;
+  const SimPlan &p = b->slots[slot].plan;
+  const BatchInst &I = b->h_tab[slot];
+  const long long N = p.geo.N;
+  if (count != (size_t)p.NVAR * (size_t)N) return bfail(b, SMAUG_ERR_ARG, "state must hold NVAR * N doubles");
+  BK(cudaSetDevice(b->device));
+  if (p.mixed) {
+    combine_kernel<<<148 * 8, 256, 0, b->stream>>>(I.F[0], I.F[1], I.W[0], (long long)p.NW * N);
+    b->launches++;
+    BK(cudaGetLastError());
+  }
+  BK(cudaMemcpyAsync(w, I.W[0], sizeof(double) * p.NW * N, cudaMemcpyDeviceToHost, b->stream));
+  BK(cudaMemcpyAsync(w + (size_t)p.NW * N, I.bg, sizeof(double) * p.NB * N, cudaMemcpyDeviceToHost, b->stream));
+  BK(cudaStreamSynchronize(b->stream));
+  return SMAUG_OK;
+}
+
+int smaug_batch_get_scalars(smaug_batch *b, int slot, double out[8]) {
+  if (!b || !out || slot < 0 || slot >= b->max_inst || !b->slots[slot].used) return SMAUG_ERR_ARG;
+  BK(cudaSetDevice(b->device));
+  DevScalars s;
+  long long left = 0;
+  BK(cudaMemcpyAsync(&s, b->h_tab[slot].sc, sizeof(DevScalars), cudaMemcpyDeviceToHost, b->stream));
+  BK(cudaMemcpyAsync(&left, b->d_left + slot, sizeof(long long), cudaMemcpyDeviceToHost, b->stream));
+  BK(cudaStreamSynchronize(b->stream));
+  out[0] = s.dt;
+  out[1] = s.maxcourant;
+  out[2] = s.maxviscoef;
+  out[3] = s.dtdiffvisc;
+  for (int d = 0; d < 3; ++d) out[4 + d] = d < b->D ? red_get(s.red[0], d) : 0.0;
+  out[7] = (double)(b->slots[slot].steps_total - left);
+  return SMAUG_OK;
+}
+
+int smaug_batch_tune(smaug_batch *b, int reps, int *variant_out, double *ms_out, int nms) {
+  if (!b || reps < 1) return SMAUG_ERR_ARG;
+  BK(cudaSetDevice(b->device));
+  const int nv = b->D == 2 ? kBatchVariants2 : kBatchVariants3;
+  cudaEvent_t e0, e1;
+  BK(cudaEventCreate(&e0));
+  BK(cudaEventCreate(&e1));
+  int best = b->variant;
+  float best_ms = 1e30f;
+  for (int v = 0; v < nv; ++v) {
+    b->variant = v;
+    int rc = rebuild(b);
+    if (rc != SMAUG_OK) return rc;
+    if (b->nwork == 0) break;
+    batch_go_kernel<<<(b->max_inst + 127) / 128, 128, 0, b->stream>>>(b->d_tab, b->max_inst);
+    smaug_batchk::launch_batch_stage(b->D, b->mixed, v, b->d_tab, b->d_work, b->nwork, 1, b->grid, b->stream);
+    BK(cudaEventRecord(e0, b->stream));
+    for (int r = 0; r < reps; ++r)
+      smaug_batchk::launch_batch_stage(b->D, b->mixed, v, b->d_tab, b->d_work, b->nwork, 1, b->grid, b->stream);
+    BK(cudaEventRecord(e1, b->stream));
+    BK(cudaEventSynchronize(e1));
+    float ms = 0.f;
+    BK(cudaEventElapsedTime(&ms, e0, e1));
+    ms /= reps;
+    b->launches += reps + 2;
+    if (ms_out && v < nms) ms_out[v] = ms;
+    if (ms < best_ms) {
+      best_ms = ms;
+      best = v;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  b->variant = best;
+  b->dirty = true;
+  if (variant_out) *variant_out = best;
+  return SMAUG_OK;
+}
+
+int smaug_batch_set_variant(smaug_batch *b, int variant) {
+  if (!b) return SMAUG_ERR_ARG;
+  const int nv = b->D == 2 ? kBatchVariants2 : kBatchVariants3;
+  if (variant < 0 || variant >= nv) return bfail(b, SMAUG_ERR_ARG, "no such tile variant");
+  b->variant = variant;
+  b->dirty = true;
+  return SMAUG_OK;
+}
+
+int smaug_batch_info(smaug_batch *b, size_t *free_bytes, size_t *largest_free, int *sims) {
+  if (!b) return SMAUG_ERR_ARG;
+  size_t tot = 0, big = 0;
+  for (auto &f : b->free_) {
+    tot += f.second;
+    big = std::max(big, f.second);
+  }
+  int n = 0;
+  for (auto &s : b->slots) n += s.used;
+  if (free_bytes) *free_bytes = tot;
+  if (largest_free) *largest_free = big;
+  if (sims) *sims = n;
+  return SMAUG_OK;
+}
+
+int smaug_batch_profile_stages(smaug_batch *b, int enable) {
+  if (!b) return SMAUG_ERR_ARG;
+  b->profile = enable != 0;
+  b->ev_used = 0;
+  return SMAUG_OK;
+}
+
+int smaug_batch_stage_times(smaug_batch *b, double *ms_total, long long *count) {
+  if (!b || !ms_total || !count) return SMAUG_ERR_ARG;
+  BK(cudaSetDevice(b->device));
+  BK(cudaStreamSynchronize(b->stream));
+  double t = 0.0;
+  for (size_t i = 0; i + 1 < b->ev_used; i += 2) {
+    float ms = 0.f;
+    BK(cudaEventElapsedTime(&ms, b->ev[i], b->ev[i + 1]));
+    t += ms;
+  }
+  *ms_total = t;
+  *count = (long long)(b->ev_used / 2);
+  b->ev_used = 0;
+  return SMAUG_OK;
+}
+
+void *smaug_batch_stream(smaug_batch *b) { return b ? (void *)b->stream : nullptr; }
+long long smaug_batch_launch_count(smaug_batch *b) { return b ? b->launches : 0; }
+const char *smaug_batch_last_error(smaug_batch *b) { return b ? b->err.c_str() : "null batch"; }
+
+}  // extern "C"

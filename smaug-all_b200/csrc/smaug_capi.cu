@@ -21,19 +21,8 @@
 
 #include "../../include/smaug_b200.h"
 #include "smaug_device.cuh"
-
-namespace smaug_exact {
-void launch_stage(int D, bool mixed, const smaug::StageArgs &a, const smaug::Geo &g, const smaug::Phys &p,
-                  cudaStream_t st);
-void launch_reduce(int D, const double *w, const double *bg, const smaug::Geo &g, const smaug::Phys &p,
-                   smaug::Reduce *r, cudaStream_t st);
-}  // namespace smaug_exact
-namespace smaug_fast {
-void launch_stage(int D, bool mixed, const smaug::StageArgs &a, const smaug::Geo &g, const smaug::Phys &p,
-                  cudaStream_t st);
-void launch_reduce(int D, const double *w, const double *bg, const smaug::Geo &g, const smaug::Phys &p,
-                   smaug::Reduce *r, cudaStream_t st);
-}  // namespace smaug_fast
+#include "smaug_batch.cuh"
+#include "smaug_common.cuh"
 
 using namespace smaug;
 
@@ -41,12 +30,7 @@ namespace {
 
 // Everything one simulation's launches need: the context API and the
 // no-allocation entry point both fill one of these.
-struct Run {
-  int D = 0, NW = 0, NB = 0, NVAR = 0;
-  Geo geo{};
-  Phys phys{};
-  bool rk4 = true, exact = false, mixed = false;
-  double dt0 = 0.0;
+struct Run : SimPlan {
   cudaStream_t stream = nullptr;
   double *W[4] = {nullptr, nullptr, nullptr, nullptr};  // state, then RK stages (or ping-pong)
   // mixed precision: FP32 base value, its FP32 compensation, two FP32 stage
@@ -54,6 +38,11 @@ struct Run {
   float *F[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
   double *bg = nullptr;
   DevScalars *sc = nullptr;
+  // the production RK4 path runs the batch stage kernel over a table of this
+  // one simulation (so a simulation gives the same bits alone and in a batch)
+  BatchInst *inst = nullptr;
+  BatchInst h_inst{};
+  int ntiles = 0;
   int cur = 0;
   long long launches = 0;
   // optional per-stage timing
@@ -61,153 +50,26 @@ struct Run {
   size_t *ev_used = nullptr;
 };
 
-// ndimp of the reference's reductions (computedervfields.cu:1940-1950).
-long long ref_ndimp(long long dimp) {
-  double fn, fractn, in;
-  fn = log((double)dimp) / log(2.0);
-  fractn = modf(fn, &in);
-  if (fractn > 0) {
-    fn += 1;
-    return (long long)(int)pow(2, fn);
-  }
-  return dimp;
-}
-
-// Validate params and fill the size/physics part of a Run.  Returns an error
-// message or nullptr.
-const char *plan(const smaug_params *prm, Run &r) {
-  const int D = prm->ndim;
-  if (D != 2 && D != 3) return "ndim must be 2 or 3";
-  r.D = D;
-  r.NW = 2 + 2 * D;
-  r.NVAR = 4 + 3 * D;
-  r.NB = r.NVAR - r.NW;
-  long long N = 1;
-  for (int d = 0; d < 3; ++d) {
-    const int n = d < D ? prm->n[d] : 1;
-    if (d < D && (n < 10 || n > (1 << 20))) return "each dimension needs 10..2^20 cells including ghosts";
-    if (d < D && prm->btype[d] != SMAUG_BC_PERIODIC && prm->btype[d] != SMAUG_BC_CONTCD4)
-      return "boundary type must be periodic (0) or contcd4 (4)";
-    r.geo.n[d] = n;
-    r.geo.btype[d] = d < D ? prm->btype[d] : 0;
-    N *= n;
-  }
-  r.geo.st[0] = 1;
-  r.geo.st[1] = r.geo.n[0];
-  r.geo.st[2] = (long long)r.geo.n[0] * r.geo.n[1];
-  r.geo.N = N;
-  r.geo.K = ((ref_ndimp(N) + 511) / 512) * 64;
-  Phys &p = r.phys;
-  p.gamma = prm->gamma;
-  p.courant = prm->courant;
-  for (int f = 0; f < 13; ++f) p.chyp[f] = prm->chyp[f];
-  p.has_grav = 0;
-  for (int d = 0; d < 3; ++d) {
-    p.g[d] = d < D ? prm->g[d] : 0.0;
-    if (p.g[d] != 0.0) p.has_grav = 1;
-  }
-  p.hyperdif = prm->hyperdif;
-  p.dt_mode = prm->dt_mode;
-  p.has_bgb = 1;
-  r.rk4 = prm->rk4 != 0;
-  r.exact = prm->exact != 0;
-  r.dt0 = prm->dt0;
-  if (prm->precision != SMAUG_PREC_FP64 && prm->precision != SMAUG_PREC_MIXED)
-    return "precision must be SMAUG_PREC_FP64 (0) or SMAUG_PREC_MIXED (1)";
-  r.mixed = prm->precision == SMAUG_PREC_MIXED;
-  if (r.mixed && (!r.rk4 || r.exact)) return "mixed precision needs rk4 = 1 and exact = 0";
-  return nullptr;
-}
-
-// Ghost fill of the evolved fields from their interior sources (periodic /
-// contcd4), used when a state is loaded (iosmaug.cpp:786-794).
-__global__ void ghost_fill_kernel(double *w, int nw, Geo g, int D) {
-  for (long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x; j < g.N; j += (long long)gridDim.x * blockDim.x) {
-    long long r = j;
-    int c[3] = {0, 0, 0};
-    c[0] = (int)(r % g.n[0]);
-    r /= g.n[0];
-    c[1] = (int)(r % g.n[1]);
-    c[2] = (int)(r / g.n[1]);
-    int s[3] = {c[0], c[1], c[2]};
-    bool ghost = false;
-    for (int d = 0; d < D; ++d) {
-      const int n = g.n[d], x = c[d];
-      if (x >= 2 && x <= n - 3) continue;
-      ghost = true;
-      if (g.btype[d] == 0)
-        s[d] = x < 2 ? x + (n - 4) : x - (n - 4);
-      else
-        s[d] = x == 0 ? 4 : x == 1 ? 3 : x == n - 1 ? n - 5 : n - 4;
-    }
-    if (!ghost) continue;
-    const long long src = s[0] + (long long)s[1] * g.st[1] + (long long)s[2] * g.st[2];
-    for (int f = 0; f < nw; ++f) w[(long long)f * g.N + j] = w[(long long)f * g.N + src];
-  }
-}
-
-// The moddton dt block of the reference loop (iosmaug.cpp:855-898):
-// dt = courant / maxcourant, then for n > 1 the viscous limit of cugetdtvisc1
-// (nushk1.cu:658-790) as that routine actually evaluates it: its buffer holds
-// maxviscoef/delx^2 on the first K cells and the courant values c_f/delx of
-// the last dimension on the rest.
 __global__ void dt_kernel(DevScalars *sc, Phys p, int D) {
-  if (threadIdx.x != 0 || blockIdx.x != 0) return;
-  sc->step += 1;
-  const int n = sc->step;
-  if (p.dt_mode == 1) {
-    const double maxc = red_get(sc->red[0], 3);
-    sc->maxcourant = maxc;
-    if (((p.courant) / (maxc)) > 1.0e-8) sc->dt = (p.courant) / (maxc);
-    if (n > 1) {
-      const double cpred = red_get(sc->red[0], 4);
-      double dtd = 0.0000000001;
-      for (int dir = 0; dir < D; ++dir) {
-        double m = cpred;
-        double v = ((sc->maxviscoef) + 0.0) / (sc->minsq[dir]);
-        if (v > m) m = v;
-        if (m > dtd) dtd = m;
-        dtd = 0.25 / dtd;
-      }
-      sc->dtdiffvisc = dtd;
-    }
-    if ((sc->dtdiffvisc) > 1.0e-8 && (sc->dt) > ((sc->dtdiffvisc))) sc->dt = sc->dtdiffvisc;
+  if (threadIdx.x == 0 && blockIdx.x == 0) {
+    dt_update(sc, p, D);
+    sc->go = 1;
   }
-  if (!isfinite(sc->dt) || sc->dt <= 0.0) sc->status = SMAUG_ERR_NONFINITE;
-  for (int s = 1; s < 5; ++s)
-    for (int k = 0; k < 8; ++k) sc->red[s].v[k] = 0ull;
 }
 
-// End of step: running maximum of the hyperviscosity (the reference's reset
-// is undone by cucomputec's params copy, computedervfields.cu:2298-2328) and
-// carry the maxima of the new state to slot 0.
 __global__ void finish_kernel(DevScalars *sc, int last) {
-  if (threadIdx.x != 0 || blockIdx.x != 0) return;
-  double nu = 0.0;
-  for (int s = 1; s <= last; ++s) nu = fmax(nu, red_get(sc->red[s], 5));
-  if (nu > sc->maxviscoef) sc->maxviscoef = nu;
-  sc->red[0] = sc->red[last];
-  for (int k = 0; k < 6; ++k) {
-    double v = red_get(sc->red[0], k);
-    if (!isfinite(v)) sc->status = SMAUG_ERR_NONFINITE;
-  }
+  if (threadIdx.x == 0 && blockIdx.x == 0) finish_update(sc, last);
 }
 
-// Fresh run state: dt0, counters and maxima cleared (minsq kept: it belongs
-// to the metric).
 __global__ void reset_scalars_kernel(DevScalars *sc, double dt0) {
-  if (threadIdx.x != 0 || blockIdx.x != 0) return;
-  sc->dt = dt0;
-  sc->dtdiffvisc = 0.0;
-  sc->maxviscoef = 0.0;
-  sc->maxcourant = 0.0;
-  sc->step = 0;
-  sc->status = 0;
-  for (int s = 0; s < 5; ++s)
-    for (int k = 0; k < 8; ++k) sc->red[s].v[k] = 0ull;
+  if (threadIdx.x == 0 && blockIdx.x == 0) reset_update(sc, dt0);
 }
 
-void launch_stage(Run &r, const StageArgs &a) {
+const char *plan(const smaug_params *prm, Run &r) { return plan_sim(prm, r); }
+
+// Launch one stage kernel, bracketed by timing events when profiling is on.
+template <typename F>
+void timed_launch(Run &r, F launch) {
   cudaEvent_t e1 = nullptr;
   if (r.ev && r.ev_used) {
     while (r.ev->size() < *r.ev_used + 2) {
@@ -221,29 +83,49 @@ void launch_stage(Run &r, const StageArgs &a) {
       *r.ev_used += 2;
     }
   }
-  if (r.exact)
-    smaug_exact::launch_stage(r.D, false, a, r.geo, r.phys, r.stream);
-  else
-    smaug_fast::launch_stage(r.D, r.mixed, a, r.geo, r.phys, r.stream);
+  launch();
   if (e1) cudaEventRecord(e1, r.stream);
   r.launches++;
 }
 
-// FP64 state -> FP32 value + FP32 compensation (w = hi + lo to ~48 bits).
-__global__ void split_kernel(const double *__restrict__ w, float *__restrict__ hi, float *__restrict__ lo, long long n) {
-  for (long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x; j < n; j += (long long)gridDim.x * blockDim.x) {
-    const double v = w[j];
-    const float h = (float)v;
-    hi[j] = h;
-    lo[j] = (float)(v - (double)h);
-  }
+void launch_stage(Run &r, const StageArgs &a) {
+  timed_launch(r, [&] {
+    if (r.exact)
+      smaug_exact::launch_stage(r.D, false, a, r.geo, r.phys, r.stream);
+    else
+      smaug_fast::launch_stage(r.D, r.mixed, a, r.geo, r.phys, r.stream);
+  });
 }
 
-// FP32 value + compensation -> FP64 state.
-__global__ void combine_kernel(const float *__restrict__ hi, const float *__restrict__ lo, double *__restrict__ w,
-                               long long n) {
-  for (long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x; j < n; j += (long long)gridDim.x * blockDim.x)
-    w[j] = (double)hi[j] + (double)lo[j];
+// RK stage k (1..4) of the production path: the batch stage kernel, one
+// block per tile of this simulation.
+void launch_rk_stage(Run &r, int k) {
+  timed_launch(r, [&] {
+    smaug_batchk::launch_batch_stage(r.D, r.mixed, 0, r.inst, nullptr, r.ntiles, k, r.ntiles, r.stream);
+  });
+}
+
+// Describe the simulation to the batch stage kernel (production RK4 path).
+// Called whenever the metric, the backgrounds or the buffers change.
+cudaError_t run_upload_inst(Run &r) {
+  if (!r.rk4 || r.exact || !r.inst) return cudaSuccess;
+  BatchInst &I = r.h_inst;
+  I = BatchInst{};
+  I.geo = r.geo;
+  I.phys = r.phys;
+  I.bg = r.bg;
+  for (int k = 0; k < 4; ++k) I.W[k] = r.W[k];
+  for (int k = 0; k < 5; ++k) I.F[k] = r.F[k];
+  I.sc = r.sc;
+  I.active = 1;
+  int t[3];
+  batch_tile_shape(r.D, 0, t);
+  r.ntiles = 1;
+  for (int d = 0; d < 3; ++d) {
+    I.tiles[d] = d < r.D ? (r.geo.n[d] - 4 + t[d] - 1) / t[d] : 1;
+    r.ntiles *= I.tiles[d];
+  }
+  return cudaMemcpyAsync(r.inst, &I, sizeof(BatchInst), cudaMemcpyHostToDevice, r.stream);
 }
 
 // A state is in r.W[0] (evolved) and r.bg: fill ghosts, reset scalars,
@@ -285,37 +167,33 @@ cudaError_t run_steps(Run &r, int nsteps) {
     if (r.mixed) {
       // the same fourstep with FP32 stage states: S1 = W + dt/2 L(W),
       // S2 = W + dt/2 L(S1), S3 = W + dt L(S2), A = (S1 + 2 S2 + S3 - 4 W)/3
-      // accumulated stage by stage, W <- W + dt/6 L(S3) + A
-      float *w32 = r.F[0], *c32 = r.F[1], *sa = r.F[2], *sb = r.F[3], *acc = r.F[4];
-      a.w32 = w32; a.c32 = c32; a.acc32 = acc;
-      a.in32 = w32; a.out32 = sa; a.kind = 1; a.red_in = 0; a.red_out = 1; a.hdiv = 2.0;
-      launch_stage(r, a);
-      a.in32 = sa;  a.out32 = sb; a.kind = 2; a.red_in = 1; a.red_out = 2; a.hdiv = 2.0;
-      launch_stage(r, a);
-      a.in32 = sb;  a.out32 = sa; a.kind = 3; a.red_in = 2; a.red_out = 3; a.hdiv = 1.0;
-      launch_stage(r, a);
-      a.in32 = sa;  a.out32 = nullptr; a.kind = 4; a.red_in = 3; a.red_out = 4; a.hdiv = 6.0;
-      launch_stage(r, a);
+      // accumulated stage by stage, W <- W + dt/6 L(S3) + A (stage roles in
+      // batch_args, batch_kernels.cu)
+      for (int k = 1; k <= 4; ++k) launch_rk_stage(r, k);
       finish_kernel<<<1, 1, 0, r.stream>>>(r.sc, 4);
     } else if (!r.rk4) {
       double *w = r.W[r.cur], *o = r.W[1 - r.cur];
       a.in = w; a.base = w; a.out = o; a.acc = nullptr; a.kind = 0;
-      a.red_in = 0; a.red_out = 1; a.hdiv = 1.0;
+      a.red_in = 0; a.red_out = 1; a.hdiv = 1.0; a.tfrac = 0.0;
       launch_stage(r, a);
       finish_kernel<<<1, 1, 0, r.stream>>>(r.sc, 1);
       r.cur = 1 - r.cur;
+    } else if (!r.exact) {
+      // production FP64 fourstep: the same stage roles in the batch kernel
+      for (int k = 1; k <= 4; ++k) launch_rk_stage(r, k);
+      finish_kernel<<<1, 1, 0, r.stream>>>(r.sc, 4);
     } else {
       // SAC fourstep (vac.t:447-462): W1 = W + dt/2 L(W); W2 = W + dt/2 L(W1);
       // W3 = W + dt L(W2) and W1 <- (W1 + 2 W2 + W3 - 4 W)/3; W <- (W + dt/6 L(W3)) + W1
       double *W = r.W[0], *W1 = r.W[1], *W2 = r.W[2], *W3 = r.W[3];
       a.base = W;
-      a.in = W;  a.out = W1; a.acc = nullptr; a.kind = 0; a.red_in = 0; a.red_out = 1; a.hdiv = 2.0;
+      a.in = W;  a.out = W1; a.acc = nullptr; a.kind = 0; a.red_in = 0; a.red_out = 1; a.hdiv = 2.0; a.tfrac = 0.0;
       launch_stage(r, a);
-      a.in = W1; a.out = W2; a.red_in = 1; a.red_out = 2; a.hdiv = 2.0;
+      a.in = W1; a.out = W2; a.red_in = 1; a.red_out = 2; a.hdiv = 2.0; a.tfrac = 0.5;
       launch_stage(r, a);
-      a.in = W2; a.out = W3; a.acc = W1; a.kind = 3; a.red_in = 2; a.red_out = 3; a.hdiv = 1.0;
+      a.in = W2; a.out = W3; a.acc = W1; a.kind = 3; a.red_in = 2; a.red_out = 3; a.hdiv = 1.0; a.tfrac = 0.5;
       launch_stage(r, a);
-      a.in = W3; a.out = W;  a.acc = W1; a.kind = 4; a.red_in = 3; a.red_out = 4; a.hdiv = 6.0;
+      a.in = W3; a.out = W;  a.acc = W1; a.kind = 4; a.red_in = 3; a.red_out = 4; a.hdiv = 6.0; a.tfrac = 1.0;
       launch_stage(r, a);
       finish_kernel<<<1, 1, 0, r.stream>>>(r.sc, 4);
     }
@@ -372,43 +250,6 @@ __global__ void minsq_init_kernel(DevScalars *sc) {
     for (int d = 0; d < 3; ++d) sc->minsq[d] = INFINITY;
 }
 
-// 1-D metric lines, tensor-product check and min delx^2 over the first K
-// cells, from a host metric (ndim * N doubles).  Returns an error or nullptr.
-const char *metric_host(const Run &r, const double *delx, double *d1, double minsq[3]) {
-  const int D = r.D;
-  const long long N = r.geo.N;
-  size_t off = 0;
-  for (int d = 0; d < 3; ++d) minsq[d] = INFINITY;
-  for (int d = 0; d < D; ++d) {
-    const double *m = delx + (size_t)d * N;
-    const int n = r.geo.n[d];
-    for (int x = 0; x < n; ++x) {
-      int c[3] = {2, 2, D == 3 ? 2 : 0};
-      c[d] = x;
-      d1[off + x] = m[c[0] + c[1] * r.geo.st[1] + c[2] * r.geo.st[2]];
-    }
-    for (long long j = 0; j < N; ++j) {
-      long long q = j;
-      int c[3];
-      c[0] = (int)(q % r.geo.n[0]);
-      q /= r.geo.n[0];
-      c[1] = (int)(q % r.geo.n[1]);
-      c[2] = (int)(q / r.geo.n[1]);
-      bool inner = true;
-      for (int e = 0; e < D; ++e)
-        if (c[e] < 2 || c[e] > r.geo.n[e] - 3) inner = false;
-      if (inner && m[j] != d1[off + c[d]]) return "metric is not a tensor-product grid on the inner cells";
-      if (!(m[j] > 0.0)) return "metric entries must be positive";
-      if (j < r.geo.K) {
-        const double v = (m[j]) * (m[j]);
-        if (v < minsq[d]) minsq[d] = v;
-      }
-    }
-    off += n;
-  }
-  return nullptr;
-}
-
 }  // namespace
 
 struct smaug_ctx {
@@ -416,6 +257,7 @@ struct smaug_ctx {
   int device = 0;
   Run run;
   double *dx1 = nullptr;     // concatenated 1-D metric
+  double *drv = nullptr;     // driver factor lines
   double *dxlast = nullptr;  // full metric of the last dim
   bool have_metric = false, have_state = false;
   long long steps = 0;
@@ -464,6 +306,20 @@ int smaug_create(const smaug_params *prm, int device, smaug_ctx **out) {
   CK(cudaMalloc(&ctx->dx1, sizeof(double) * (r.geo.n[0] + r.geo.n[1] + r.geo.n[2])));
   CK(cudaMalloc(&ctx->dxlast, fsz));
   CK(cudaMalloc(&r.sc, sizeof(DevScalars)));
+  CK(cudaMalloc(&r.inst, sizeof(BatchInst)));
+  {
+    const size_t nl = (size_t)r.geo.n[0] + r.geo.n[1] + r.geo.n[2];
+    std::vector<double> lines(nl);
+    driver_lines(r, prm, lines.data());
+    CK(cudaMalloc(&ctx->drv, sizeof(double) * nl));
+    CK(cudaMemcpyAsync(ctx->drv, lines.data(), sizeof(double) * nl, cudaMemcpyHostToDevice, r.stream));
+    CK(cudaStreamSynchronize(r.stream));
+    size_t off = 0;
+    for (int d = 0; d < 3; ++d) {
+      r.geo.drvf[d] = ctx->drv + off;
+      off += r.geo.n[d];
+    }
+  }
   CK(cudaMemsetAsync(r.sc, 0, sizeof(DevScalars), r.stream));
   CK(cudaStreamSynchronize(r.stream));
   return SMAUG_OK;
@@ -478,8 +334,10 @@ int smaug_destroy(smaug_ctx *ctx) {
   for (auto &f : r.F) cudaFree(f);
   cudaFree(r.bg);
   cudaFree(ctx->dx1);
+  cudaFree(ctx->drv);
   cudaFree(ctx->dxlast);
   cudaFree(r.sc);
+  cudaFree(r.inst);
   for (auto e : ctx->ev) cudaEventDestroy(e);
   if (r.stream) cudaStreamDestroy(r.stream);
   delete ctx;
@@ -509,6 +367,7 @@ int smaug_set_metric(smaug_ctx *ctx, const double *delx, size_t count) {
                      r.stream));
   r.geo.dxlast = ctx->dxlast;
   CK(cudaMemcpyAsync(r.sc->minsq, minsq, sizeof(minsq), cudaMemcpyHostToDevice, r.stream));
+  CK(run_upload_inst(r));
   CK(cudaStreamSynchronize(r.stream));
   ctx->have_metric = true;
   return SMAUG_OK;
@@ -537,6 +396,7 @@ static int load_state(smaug_ctx *ctx, const double *w, size_t count, cudaMemcpyK
     r.phys.has_bgb = 1;
   }
   CK(run_load(r));
+  CK(run_upload_inst(r));
   CK(cudaStreamSynchronize(r.stream));
   ctx->have_state = true;
   ctx->steps = 0;
@@ -686,10 +546,10 @@ int smaug_step_noalloc(const smaug_params *prm, const double *delx_dev, const do
     return SMAUG_ERR_ARG;
   }
   const long long N = r.geo.N;
-  const size_t head = (sizeof(DevScalars) + 255) / 256 * 256;
+  const size_t head = (sizeof(DevScalars) + 255) / 256 * 256 + (sizeof(BatchInst) + 255) / 256 * 256;
   const size_t lines = ((size_t)(r.geo.n[0] + r.geo.n[1] + r.geo.n[2]) * sizeof(double) + 255) / 256 * 256;
   const size_t field = ((size_t)r.NW * (size_t)N * sizeof(double) + 255) / 256 * 256;
-  const size_t need = head + lines + 3 * field;
+  const size_t need = head + 2 * lines + 3 * field;  // metric lines, driver lines, RK buffers
   if (need > (size_t)SMAUG_NOALLOC_SCRATCH_BYTES) {
     char msg[160];
     std::snprintf(msg, sizeof(msg), "grid needs %zu bytes of scratch, above the %u-byte maximum of smaug_step_noalloc",
@@ -706,17 +566,26 @@ int smaug_step_noalloc(const smaug_params *prm, const double *delx_dev, const do
   unsigned char *s = (unsigned char *)base;
   r.stream = (cudaStream_t)stream;
   r.sc = (DevScalars *)s;
+  r.inst = (BatchInst *)(s + (sizeof(DevScalars) + 255) / 256 * 256);
   double *dx1 = (double *)(s + head);
   r.W[0] = w_out_dev;
   r.bg = w_out_dev + (size_t)r.NW * N;
-  for (int k = 0; k < 3; ++k) r.W[1 + k] = (double *)(s + head + lines + k * field);
+  double *drv = (double *)(s + head + lines);
+  for (int k = 0; k < 3; ++k) r.W[1 + k] = (double *)(s + head + 2 * lines + k * field);
   size_t off = 0;
   for (int d = 0; d < r.D; ++d) {
     r.geo.dx1[d] = dx1 + off;
     off += r.geo.n[d];
   }
   r.geo.dxlast = delx_dev + (size_t)(r.D - 1) * N;
+  off = 0;
+  for (int d = 0; d < 3; ++d) {
+    r.geo.drvf[d] = drv + off;
+    off += r.geo.n[d];
+  }
   r.phys.has_bgb = 1;
+  std::vector<double> drv_host((size_t)r.geo.n[0] + r.geo.n[1] + r.geo.n[2]);
+  driver_lines(r, prm, drv_host.data());
 #define NA(call)                                \
   do {                                          \
     cudaError_t e_ = (call);                    \
@@ -729,7 +598,9 @@ int smaug_step_noalloc(const smaug_params *prm, const double *delx_dev, const do
     NA(cudaMemcpyAsync(w_out_dev, w_in_dev, sizeof(double) * (size_t)r.NVAR * N, cudaMemcpyDeviceToDevice, r.stream));
   // every call starts from cleared scalars: the array keeps the last call's data
   NA(cudaMemsetAsync(r.sc, 0, sizeof(DevScalars), r.stream));
+  NA(cudaMemcpyAsync(drv, drv_host.data(), sizeof(double) * drv_host.size(), cudaMemcpyHostToDevice, r.stream));
   NA(run_load(r));  // ghost fill of w_out, scalars reset, initial maxima
+  NA(run_upload_inst(r));
   minsq_init_kernel<<<1, 1, 0, r.stream>>>(r.sc);
   metric_kernel<<<148 * 4, 256, 0, r.stream>>>(delx_dev, r.geo, r.D, dx1, r.sc);
   NA(cudaGetLastError());

@@ -1,0 +1,266 @@
+// smaug_common.cuh -- host planning and device scalar logic shared by the
+// single-simulation context (smaug_capi.cu) and the batch (smaug_batch.cu).
+// Everything here has internal linkage in each translation unit.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cmath>
+
+#include "../../include/smaug_b200.h"
+#include "smaug_device.cuh"
+
+// stage kernels of the two builds (stage_exact.cu, stage_fast.cu)
+namespace smaug_exact {
+void launch_stage(int D, bool mixed, const smaug::StageArgs &a, const smaug::Geo &g, const smaug::Phys &p,
+                  cudaStream_t st);
+void launch_reduce(int D, const double *w, const double *bg, const smaug::Geo &g, const smaug::Phys &p,
+                   smaug::Reduce *r, cudaStream_t st);
+}  // namespace smaug_exact
+namespace smaug_fast {
+void launch_stage(int D, bool mixed, const smaug::StageArgs &a, const smaug::Geo &g, const smaug::Phys &p,
+                  cudaStream_t st);
+void launch_reduce(int D, const double *w, const double *bg, const smaug::Geo &g, const smaug::Phys &p,
+                   smaug::Reduce *r, cudaStream_t st);
+}  // namespace smaug_fast
+
+using namespace smaug;
+namespace {
+
+// Sizes, physics and options of one simulation, from its smaug_params.
+struct SimPlan {
+  int D = 0, NW = 0, NB = 0, NVAR = 0;
+  Geo geo{};
+  Phys phys{};
+  bool rk4 = true, exact = false, mixed = false;
+  double dt0 = 0.0;
+};
+
+// ndimp of the reference's reductions (computedervfields.cu:1940-1950).
+long long ref_ndimp(long long dimp) {
+  double fn, fractn, in;
+  fn = log((double)dimp) / log(2.0);
+  fractn = modf(fn, &in);
+  if (fractn > 0) {
+    fn += 1;
+    return (long long)(int)pow(2, fn);
+  }
+  return dimp;
+}
+
+// Validate params and fill a SimPlan.  Returns an error message or nullptr.
+const char *plan_sim(const smaug_params *prm, SimPlan &r) {
+  const int D = prm->ndim;
+  if (D != 2 && D != 3) return "ndim must be 2 or 3";
+  r.D = D;
+  r.NW = 2 + 2 * D;
+  r.NVAR = 4 + 3 * D;
+  r.NB = r.NVAR - r.NW;
+  long long N = 1;
+  for (int d = 0; d < 3; ++d) {
+    const int n = d < D ? prm->n[d] : 1;
+    if (d < D && (n < 10 || n > (1 << 20))) return "each dimension needs 10..2^20 cells including ghosts";
+    if (d < D && prm->btype[d] != SMAUG_BC_PERIODIC && prm->btype[d] != SMAUG_BC_CONTCD4)
+      return "boundary type must be periodic (0) or contcd4 (4)";
+    r.geo.n[d] = n;
+    r.geo.btype[d] = d < D ? prm->btype[d] : 0;
+    N *= n;
+  }
+  r.geo.st[0] = 1;
+  r.geo.st[1] = r.geo.n[0];
+  r.geo.st[2] = (long long)r.geo.n[0] * r.geo.n[1];
+  r.geo.N = N;
+  r.geo.K = ((ref_ndimp(N) + 511) / 512) * 64;
+  Phys &p = r.phys;
+  p.gamma = prm->gamma;
+  p.courant = prm->courant;
+  for (int f = 0; f < 13; ++f) p.chyp[f] = prm->chyp[f];
+  p.has_grav = 0;
+  for (int d = 0; d < 3; ++d) {
+    p.g[d] = d < D ? prm->g[d] : 0.0;
+    if (p.g[d] != 0.0) p.has_grav = 1;
+  }
+  p.hyperdif = prm->hyperdif;
+  p.dt_mode = prm->dt_mode;
+  p.drv_on = prm->drv_on != 0;
+  p.drv_dir = prm->drv_dir;
+  p.drv_amp = prm->drv_amp;
+  p.drv_period = prm->drv_period;
+  if (p.drv_on) {
+    if (prm->drv_dir < 0 || prm->drv_dir >= D) return "drv_dir must name a momentum component (0..ndim-1)";
+    if (!(prm->drv_period >= 0.0)) return "drv_period must be >= 0";
+    for (int d = 0; d < D; ++d)
+      if (!(prm->dx[d] > 0.0) || !(prm->drv_width[d] >= 0.0)) return "driver needs dx > 0 and widths >= 0";
+  }
+  p.has_bgb = 1;
+  r.rk4 = prm->rk4 != 0;
+  r.exact = prm->exact != 0;
+  r.dt0 = prm->dt0;
+  if (prm->precision != SMAUG_PREC_FP64 && prm->precision != SMAUG_PREC_MIXED)
+    return "precision must be SMAUG_PREC_FP64 (0) or SMAUG_PREC_MIXED (1)";
+  r.mixed = prm->precision == SMAUG_PREC_MIXED;
+  if (r.mixed && (!r.rk4 || r.exact)) return "mixed precision needs rk4 = 1 and exact = 0";
+  return nullptr;
+}
+
+// Ghost fill of the evolved fields from their interior sources (periodic /
+// contcd4), used when a state is loaded (iosmaug.cpp:786-794).
+__global__ void ghost_fill_kernel(double *w, int nw, Geo g, int D) {
+  for (long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x; j < g.N; j += (long long)gridDim.x * blockDim.x) {
+    long long r = j;
+    int c[3] = {0, 0, 0};
+    c[0] = (int)(r % g.n[0]);
+    r /= g.n[0];
+    c[1] = (int)(r % g.n[1]);
+    c[2] = (int)(r / g.n[1]);
+    int s[3] = {c[0], c[1], c[2]};
+    bool ghost = false;
+    for (int d = 0; d < D; ++d) {
+      const int n = g.n[d], x = c[d];
+      if (x >= 2 && x <= n - 3) continue;
+      ghost = true;
+      if (g.btype[d] == 0)
+        s[d] = x < 2 ? x + (n - 4) : x - (n - 4);
+      else
+        s[d] = x == 0 ? 4 : x == 1 ? 3 : x == n - 1 ? n - 5 : n - 4;
+    }
+    if (!ghost) continue;
+    const long long src = s[0] + (long long)s[1] * g.st[1] + (long long)s[2] * g.st[2];
+    for (int f = 0; f < nw; ++f) w[(long long)f * g.N + j] = w[(long long)f * g.N + src];
+  }
+}
+
+// The moddton dt block of the reference loop (iosmaug.cpp:855-898):
+// dt = courant / maxcourant, then for n > 1 the viscous limit of cugetdtvisc1
+// (nushk1.cu:658-790) as that routine actually evaluates it: its buffer holds
+// maxviscoef/delx^2 on the first K cells and the courant values c_f/delx of
+// the last dimension on the rest.
+__device__ __forceinline__ void dt_update(DevScalars *sc, const Phys &p, int D) {
+  sc->step += 1;
+  const int n = sc->step;
+  if (p.dt_mode == 1) {
+    const double maxc = red_get(sc->red[0], 3);
+    sc->maxcourant = maxc;
+    if (((p.courant) / (maxc)) > 1.0e-8) sc->dt = (p.courant) / (maxc);
+    if (n > 1) {
+      const double cpred = red_get(sc->red[0], 4);
+      double dtd = 0.0000000001;
+      for (int dir = 0; dir < D; ++dir) {
+        double m = cpred;
+        double v = ((sc->maxviscoef) + 0.0) / (sc->minsq[dir]);
+        if (v > m) m = v;
+        if (m > dtd) dtd = m;
+        dtd = 0.25 / dtd;
+      }
+      sc->dtdiffvisc = dtd;
+    }
+    if ((sc->dtdiffvisc) > 1.0e-8 && (sc->dt) > ((sc->dtdiffvisc))) sc->dt = sc->dtdiffvisc;
+  }
+  if (!isfinite(sc->dt) || sc->dt <= 0.0) sc->status = SMAUG_ERR_NONFINITE;
+  for (int s = 1; s < 5; ++s)
+    for (int k = 0; k < 8; ++k) sc->red[s].v[k] = 0ull;
+}
+
+// End of step: running maximum of the hyperviscosity (the reference's reset
+// is undone by cucomputec's params copy, computedervfields.cu:2298-2328) and
+// carry the maxima of the new state to slot 0.
+__device__ __forceinline__ void finish_update(DevScalars *sc, int last) {
+  double nu = 0.0;
+  for (int s = 1; s <= last; ++s) nu = fmax(nu, red_get(sc->red[s], 5));
+  if (nu > sc->maxviscoef) sc->maxviscoef = nu;
+  sc->red[0] = sc->red[last];
+  for (int k = 0; k < 6; ++k) {
+    double v = red_get(sc->red[0], k);
+    if (!isfinite(v)) sc->status = SMAUG_ERR_NONFINITE;
+  }
+  sc->t += sc->dt;  // simulation time of the next step
+}
+
+// Fresh run state: dt0, counters and maxima cleared (minsq kept: it belongs
+// to the metric).
+__device__ __forceinline__ void reset_update(DevScalars *sc, double dt0) {
+  sc->dt = dt0;
+  sc->t = 0.0;
+  sc->dtdiffvisc = 0.0;
+  sc->maxviscoef = 0.0;
+  sc->maxcourant = 0.0;
+  sc->step = 0;
+  sc->status = 0;
+  for (int s = 0; s < 5; ++s)
+    for (int k = 0; k < 8; ++k) sc->red[s].v[k] = 0ull;
+}
+
+// FP64 state -> FP32 value + FP32 compensation (w = hi + lo to ~48 bits).
+__global__ void split_kernel(const double *__restrict__ w, float *__restrict__ hi, float *__restrict__ lo, long long n) {
+  for (long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x; j < n; j += (long long)gridDim.x * blockDim.x) {
+    const double v = w[j];
+    const float h = (float)v;
+    hi[j] = h;
+    lo[j] = (float)(v - (double)h);
+  }
+}
+
+// FP32 value + compensation -> FP64 state.
+__global__ void combine_kernel(const float *__restrict__ hi, const float *__restrict__ lo, double *__restrict__ w,
+                               long long n) {
+  for (long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x; j < n; j += (long long)gridDim.x * blockDim.x)
+    w[j] = (double)hi[j] + (double)lo[j];
+}
+
+// 1-D metric lines, tensor-product check and min delx^2 over the first K
+// cells, from a host metric (ndim * N doubles).  Returns an error or nullptr.
+const char *metric_host(const SimPlan &r, const double *delx, double *d1, double minsq[3]) {
+  const int D = r.D;
+  const long long N = r.geo.N;
+  size_t off = 0;
+  for (int d = 0; d < 3; ++d) minsq[d] = INFINITY;
+  for (int d = 0; d < D; ++d) {
+    const double *m = delx + (size_t)d * N;
+    const int n = r.geo.n[d];
+    for (int x = 0; x < n; ++x) {
+      int c[3] = {2, 2, D == 3 ? 2 : 0};
+      c[d] = x;
+      d1[off + x] = m[c[0] + c[1] * r.geo.st[1] + c[2] * r.geo.st[2]];
+    }
+    for (long long j = 0; j < N; ++j) {
+      long long q = j;
+      int c[3];
+      c[0] = (int)(q % r.geo.n[0]);
+      q /= r.geo.n[0];
+      c[1] = (int)(q % r.geo.n[1]);
+      c[2] = (int)(q / r.geo.n[1]);
+      bool inner = true;
+      for (int e = 0; e < D; ++e)
+        if (c[e] < 2 || c[e] > r.geo.n[e] - 3) inner = false;
+      if (inner && m[j] != d1[off + c[d]]) return "metric is not a tensor-product grid on the inner cells";
+      if (!(m[j] > 0.0)) return "metric entries must be positive";
+      if (j < r.geo.K) {
+        const double v = (m[j]) * (m[j]);
+        if (v < minsq[d]) minsq[d] = v;
+      }
+    }
+    off += n;
+  }
+  return nullptr;
+}
+
+// Driver factor lines (n0 + n1 + n2 doubles): along each dim d,
+// exp(-(x - c_d)^2 / (w_d * w_d)) at x = xmin_d + i * dx_d, or 1 where w_d = 0
+// (usersource.cu.spicule1:77-86; the oracle evaluates the same expression).
+void driver_lines(const SimPlan &r, const smaug_params *prm, double *out) {
+  size_t off = 0;
+  for (int d = 0; d < 3; ++d) {
+    const int n = r.geo.n[d];
+    for (int i = 0; i < n; ++i) {
+      double f = 1.0;
+      if (d < r.D && prm->drv_on && prm->drv_width[d] > 0.0) {
+        const double x = (prm->xmin[d]) + (((double)i) * (prm->dx[d]));
+        const double r2 = (x - prm->drv_center[d]) * (x - prm->drv_center[d]);
+        f = exp(-r2 / (prm->drv_width[d] * prm->drv_width[d]));
+      }
+      out[off + i] = f;
+    }
+    off += n;
+  }
+}
+
+}  // namespace

@@ -36,6 +36,9 @@ struct DevScalars {
   double minsq[3];    // min over the first K cells of delx_d^2 (viscous dt), set with the metric
   int step;
   int status;
+  int go;         // batch only: this simulation takes the current step
+  int pad_;
+  double t;       // simulation time at the start of the current step (driver)
   Reduce red[5];  // [0] state at step start, [1..3] RK stage outputs, [4] state at step end
 };
 
@@ -47,6 +50,7 @@ struct Geo {
   long long K;                // courant cells below K are excluded from the viscous-dt maximum
   const double *dx1[3];       // metric along d at inner cells (depends on c_d only)
   const double *dxlast;       // full per-cell metric of the last dim (courant reduction)
+  const double *drvf[3];      // driver: Gaussian factor per cell index along each dim
 };
 
 struct Phys {
@@ -58,6 +62,8 @@ struct Phys {
   int has_bgb;                // any background B or eb != 0 (energy background terms)
   int has_grav;
   int dt_mode;
+  int drv_on, drv_dir;        // momentum driver: on, driven momentum component
+  double drv_amp, drv_period; // amplitude, period (0: constant in time)
 };
 
 struct StageArgs {
@@ -75,6 +81,7 @@ struct StageArgs {
   int kind;            // FP64: 0 plain, 3 = RK stage 3, 4 = RK stage 4; mixed: RK stage 1..4
   int red_in, red_out; // reduction slots: cmax of `in`, maxima of `out`
   double hdiv;         // h = dt / hdiv (dt/2, dt/2, dt, dt/6 as the oracle divides)
+  double tfrac;        // stage input time = t + tfrac * dt (0, 1/2, 1/2, 1; driver)
 };
 
 __device__ __forceinline__ void atomic_max_nonneg(unsigned long long *slot, double v) {
@@ -262,6 +269,21 @@ __device__ __forceinline__ void visc_at(const Cell<D> &c, const Geo &g, long lon
   }
   nul = (maxt2 > 0) ? ((dx)) * (cmax) * (chyp)*maxt1 / maxt2 : 0.0;
 #undef QQ
+}
+
+// Driver velocity at inner cell c for the stage whose input is at time
+// t + tfrac * dt: A * F(c) * tdep, F = f1 * f0 (2-D) or (f1 * f0) * f2 (3-D)
+// from the host-computed factor lines, tdep = sin(2 pi t / P) or 1 (P = 0).
+// The driven momentum then gains h * vvz * (rho + rhob) of the stage output
+// (models/usersource.cu.spicule1:4-137, addsourceterms2).
+template <int D>
+__device__ __forceinline__ double driver_vvz(const Geo &g, const Phys &p, const DevScalars *sc, double tfrac,
+                                             const int *c) {
+  double f = g.drvf[1][c[1]] * g.drvf[0][c[0]];
+  if (D == 3) f = f * g.drvf[2][c[2]];
+  double tdep = 1.0;
+  if (p.drv_period > 0.0) tdep = sin(2.0 * 3.14159265358979323846 * (sc->t + tfrac * sc->dt) / p.drv_period);
+  return p.drv_amp * f * tdep;
 }
 
 }  // namespace smaug

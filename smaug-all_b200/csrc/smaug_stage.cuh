@@ -307,6 +307,13 @@ __global__ void __launch_bounds__(kBX *kBY) stage_kernel(StageArgs a, Geo g, Phy
         }
     }
 
+    // ---- momentum driver on the stage output (usersource.cu.spicule1:4-137)
+    if (p.drv_on) {
+      const double vvz = driver_vvz<D>(g, p, a.sc, a.tfrac, c);
+      const double rb = __ldg(a.bg + (long long)(L::RHOB - NW) * N + idx);
+      o[L::M0 + p.drv_dir] = o[L::M0 + p.drv_dir] + h * vvz * (o[L::RHO] + rb);
+    }
+
     // ---- Runge-Kutta combination (vac.t:447-462)
     if (a.kind == 3) {
 #pragma unroll

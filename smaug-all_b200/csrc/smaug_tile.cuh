@@ -467,6 +467,11 @@ __device__ __forceinline__ void tile_body(const StageArgs &a, const Geo &g, cons
     if (!MIXED) {
 #pragma unroll
       for (int f = 0; f < NW; ++f) o[f] = a.base[(long long)f * g.N + idx] + h * (double)dL[f];
+      if (p.drv_on) {  // momentum driver on the stage output (before the RK combination)
+        const double vvz = driver_vvz<D>(g, p, a.sc, a.tfrac, c);
+        const double rb = __ldg(a.bg + (long long)(L::RHOB - NW) * g.N + idx);
+        o[L::M0 + p.drv_dir] = o[L::M0 + p.drv_dir] + h * vvz * (o[L::RHO] + rb);
+      }
       if (a.kind == 3) {
 #pragma unroll
         for (int f = 0; f < NW; ++f) {
@@ -483,10 +488,18 @@ __device__ __forceinline__ void tile_body(const StageArgs &a, const Geo &g, cons
       //   c = 1/3, 2/3, 1/3, so A = (S1 + 2 S2 + S3 - 4 W) / 3 as the FP64 path;
       //   stage 4: W <- W + h_4 L_4 + A, kept as value + compensation.
       // Stages 1..3 round to FP32 anyway, so they take the base without c32.
+      double incs[NW];
+#pragma unroll
+      for (int f = 0; f < NW; ++f) incs[f] = h * (double)dL[f];
+      if (p.drv_on) {  // momentum driver with the stage output's density
+        const double wr = a.kind == 4 ? (double)a.w32[idx] + (double)a.c32[idx] : (double)a.w32[idx];
+        const double rb = __ldg(a.bg + (long long)(L::RHOB - NW) * g.N + idx);
+        incs[L::M0 + p.drv_dir] += h * driver_vvz<D>(g, p, a.sc, a.tfrac, c) * ((wr + incs[L::RHO]) + rb);
+      }
 #pragma unroll
       for (int f = 0; f < NW; ++f) {
         const long long j = (long long)f * g.N + idx;
-        const double inc = h * (double)dL[f];
+        const double inc = incs[f];
         if (a.kind == 4) {
           const double wn = ((double)a.w32[j] + (double)a.c32[j]) + (inc + (double)a.acc32[j]);
           hi[f] = (float)wn;

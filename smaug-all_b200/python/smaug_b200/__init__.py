@@ -27,7 +27,9 @@ SMAUG_OK = 0
 class Params(ctypes.Structure):
     _fields_ = [("ndim", _I), ("n", _I * 3), ("gamma", _D), ("courant", _D), ("chyp", _D * 13),
                 ("btype", _I * 3), ("g", _D * 3), ("hyperdif", _I), ("rk4", _I), ("dt_mode", _I),
-                ("dt0", _D), ("exact", _I), ("precision", _I)]
+                ("dt0", _D), ("exact", _I), ("precision", _I),
+                ("drv_on", _I), ("drv_dir", _I), ("drv_amp", _D), ("drv_period", _D),
+                ("drv_center", _D * 3), ("drv_width", _D * 3), ("xmin", _D * 3), ("dx", _D * 3)]
 
 
 PREC_FP64 = 0   # SMAUG_PREC_FP64
@@ -69,12 +71,69 @@ def load_library(path: Path | None = None):
     L.smaug_nvar.argtypes = [_I]
     L.smaug_profile_stages.argtypes = [ctypes.c_void_p, _I]
     L.smaug_stage_times.argtypes = [ctypes.c_void_p, _PD, ctypes.POINTER(ctypes.c_longlong)]
+    _LL = ctypes.c_longlong
+    _VP = ctypes.c_void_p
+    L.smaug_batch_footprint.argtypes = [ctypes.POINTER(Params), ctypes.POINTER(_SZ)]
+    L.smaug_batch_create.argtypes = [_I, _I, _I, _SZ, _I, ctypes.POINTER(_VP)]
+    L.smaug_batch_destroy.argtypes = [_VP]
+    L.smaug_batch_add.argtypes = [_VP, ctypes.POINTER(Params), _PD, _PD, _LL, ctypes.POINTER(_I)]
+    L.smaug_batch_remove.argtypes = [_VP, _I]
+    L.smaug_batch_step.argtypes = [_VP, _I]
+    L.smaug_batch_poll.argtypes = [_VP, ctypes.POINTER(_LL), _I]
+    L.smaug_batch_sync.argtypes = [_VP, ctypes.POINTER(_I)]
+    L.smaug_batch_get_state.argtypes = [_VP, _I, _PD, _SZ]
+    L.smaug_batch_get_scalars.argtypes = [_VP, _I, _PD]
+    L.smaug_batch_tune.argtypes = [_VP, _I, ctypes.POINTER(_I), _PD, _I]
+    L.smaug_batch_set_variant.argtypes = [_VP, _I]
+    L.smaug_batch_info.argtypes = [_VP, ctypes.POINTER(_SZ), ctypes.POINTER(_SZ), ctypes.POINTER(_I)]
+    L.smaug_batch_profile_stages.argtypes = [_VP, _I]
+    L.smaug_batch_stage_times.argtypes = [_VP, _PD, ctypes.POINTER(_LL)]
+    L.smaug_batch_stream.argtypes = [_VP]
+    L.smaug_batch_stream.restype = _VP
+    L.smaug_batch_launch_count.argtypes = [_VP]
+    L.smaug_batch_launch_count.restype = _LL
+    L.smaug_batch_last_error.argtypes = [_VP]
+    L.smaug_batch_last_error.restype = ctypes.c_char_p
     _lib = L
     return L
 
 
 def _f64(a) -> np.ndarray:
     return np.ascontiguousarray(a, dtype=np.float64)
+
+
+def make_params(prob, rk4: bool = True, dt_mode: int = 1, exact: bool = False, dt0: float = 0.0,
+                precision: int = PREC_FP64) -> Params:
+    """smaug_params for a problem (problems.Problem)."""
+    p = Params()
+    p.ndim = prob.ndim
+    for d in range(3):
+        p.n[d] = prob.n[d] if d < prob.ndim else 1
+        p.btype[d] = prob.btype[d] if d < prob.ndim else 0
+        p.g[d] = prob.g[d] if d < len(prob.g) else 0.0
+    p.gamma = prob.gamma
+    p.courant = prob.courant
+    for f in range(len(prob.chyp)):
+        p.chyp[f] = float(prob.chyp[f])
+    p.hyperdif = int(prob.hyperdif)
+    p.rk4 = int(rk4)
+    p.dt_mode = int(dt_mode)
+    p.dt0 = float(dt0)
+    p.exact = int(exact)
+    p.precision = int(precision)
+    for d in range(prob.ndim):
+        p.xmin[d] = float(prob.xmin[d])
+        p.dx[d] = float(prob.dx[d])
+    drv = getattr(prob, "driver", None)
+    if drv:
+        p.drv_on = 1
+        p.drv_dir = int(drv.get("dir", 0))
+        p.drv_amp = float(drv["amp"])
+        p.drv_period = float(drv.get("period", 0.0))
+        for d in range(prob.ndim):
+            p.drv_center[d] = float(drv["center"][d])
+            p.drv_width[d] = float(drv["width"][d])
+    return p
 
 
 class Engine:
@@ -84,22 +143,7 @@ class Engine:
                  dt0: float = 0.0, precision: int = PREC_FP64):
         self.lib = load_library()
         self.prob = prob
-        p = Params()
-        p.ndim = prob.ndim
-        for d in range(3):
-            p.n[d] = prob.n[d] if d < prob.ndim else 1
-            p.btype[d] = prob.btype[d] if d < prob.ndim else 0
-            p.g[d] = prob.g[d] if d < len(prob.g) else 0.0
-        p.gamma = prob.gamma
-        p.courant = prob.courant
-        for f in range(len(prob.chyp)):
-            p.chyp[f] = float(prob.chyp[f])
-        p.hyperdif = int(prob.hyperdif)
-        p.rk4 = int(rk4)
-        p.dt_mode = int(dt_mode)
-        p.dt0 = float(dt0)
-        p.exact = int(exact)
-        p.precision = int(precision)
+        p = make_params(prob, rk4=rk4, dt_mode=dt_mode, exact=exact, dt0=dt0, precision=precision)
         self.params = p
         h = ctypes.c_void_p()
         rc = self.lib.smaug_create(ctypes.byref(p), device, ctypes.byref(h))
@@ -169,3 +213,6 @@ class Engine:
             self.close()
         except Exception:
             pass
+
+
+from .batch import Batch, footprint  # noqa: E402,F401

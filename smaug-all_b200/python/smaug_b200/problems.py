@@ -54,6 +54,8 @@ class Problem:
     g: tuple = (0.0, 0.0, 0.0)
     hyperdif: int = 1
     meta: dict = field(default_factory=dict)
+    # momentum driver: {"dir", "amp", "period", "center", "width"} (None: off)
+    driver: dict | None = None
 
     @property
     def ncells(self) -> int:
@@ -159,6 +161,19 @@ def orszag_tang(nx: int = 256, ny: int | None = None, b0_scale: float = 1.0,
     return Problem("orszag_tang", 2, n, dx, (-NG * dx[0], -NG * dx[1]), gam, _chyp(2), (0, 0),
                    0.3, w, meta={"nx": nx, "ny": ny, "b0_scale": b0_scale, "rho_noise": rho_noise,
                                  "seed": seed})
+
+
+ENSEMBLE_SIDES = (128, 192, 256, 384, 512, 768)
+
+
+def ensemble(count: int = 96, seed: int = 4242, sides=ENSEMBLE_SIDES) -> list:
+    """Batched ensemble of independent 2-D Orszag-Tang vortices: side drawn
+    uniformly from `sides`, B0 scaled by U[0.5, 1.5], 1 % Gaussian density
+    noise per cell (noise seed = seed + instance id)."""
+    rng = np.random.default_rng(seed)
+    n = rng.choice(np.asarray(sides), size=count)
+    b0 = rng.uniform(0.5, 1.5, size=count)
+    return [orszag_tang(int(n[i]), b0_scale=float(b0[i]), rho_noise=0.01, seed=seed + i) for i in range(count)]
 
 
 def _periodic_fill(a: np.ndarray) -> np.ndarray:

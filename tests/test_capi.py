@@ -79,3 +79,44 @@ def test_create_rejects_bad_precision():
         assert lib.smaug_create(ctypes.byref(p), 0, ctypes.byref(h)) == -1
         assert b"mixed" in lib.smaug_last_error(h)
         lib.smaug_destroy(h)
+
+
+def test_batch_footprint_and_argument_checks():
+    """Batch footprints and parameter checks are host-only."""
+    from smaug_b200 import PREC_FP64, PREC_MIXED, footprint, problems
+    p = problems.orszag_tang(30)
+    N, NW, NB = p.ncells, 6, 4
+    a = lambda x: (x + 255) // 256 * 256  # noqa: E731  (arena blocks are 256-byte aligned)
+    lines = a(8 * (p.n[0] + p.n[1] + 1))
+    base = 2 * lines + a(8 * N) + a(8 * NB * N) + a(8 * NW * N)  # metric and driver lines
+    fp64 = footprint(p, PREC_FP64)
+    mixed = footprint(p, PREC_MIXED)
+    # scalars block + metric and driver lines + dxlast + backgrounds + W0, then 3 FP64 or 5 FP32 buffers
+    assert fp64 - mixed == 3 * a(8 * NW * N) - 5 * a(4 * NW * N)
+    assert fp64 > base + 3 * a(8 * NW * N) and fp64 - (base + 3 * a(8 * NW * N)) <= 1024
+    lib = load_library()
+    h = ctypes.c_void_p()
+    assert lib.smaug_batch_create(4, 0, 0, 1 << 20, 4, ctypes.byref(h)) == -1
+    assert b"ndim" in lib.smaug_batch_last_error(h)
+    lib.smaug_batch_destroy(h)
+    h = ctypes.c_void_p()
+    assert lib.smaug_batch_create(2, 5, 0, 1 << 20, 4, ctypes.byref(h)) == -1
+    lib.smaug_batch_destroy(h)
+
+
+def test_params_struct_layout_matches_header(tmp_path):
+    """The ctypes mirror of smaug_params has the C struct's size and offsets."""
+    import subprocess
+
+    from smaug_b200 import Params
+    names = [f[0] for f in Params._fields_]
+    src = tmp_path / "lay.c"
+    src.write_text('#include <stdio.h>\n#include <stddef.h>\n#include "smaug_b200.h"\nint main(void){\n'
+                   '  printf("%zu\\n", sizeof(smaug_params));\n'
+                   + "".join(f'  printf("%zu\\n", offsetof(smaug_params, {n}));\n' for n in names)
+                   + "  return 0;\n}\n")
+    exe = tmp_path / "lay"
+    subprocess.run(["gcc", "-I", str(HEADER.parent), str(src), "-o", str(exe)], check=True)
+    vals = [int(x) for x in subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split()]
+    assert vals[0] == ctypes.sizeof(Params)
+    assert vals[1:] == [getattr(Params, n).offset for n in names]
