@@ -438,6 +438,29 @@ def run_blast(a, ctx):
     return out
 
 
+def run_serving(a, ctx):
+    """Serving stream: Poisson arrivals (40/s, seed 777) of driven
+    stratified-atmosphere x-z slices, sizes {128x256 .. 512x1024}, driver
+    period U[120,600] s, amplitude U[50,500] m/s, U[200,2000] steps, mixed
+    precision, continuous batching; p50/p99 time to solution."""
+    import torch
+
+    from smaug_b200 import PREC_MIXED, Batch
+    from smaug_b200.serve import Server, atmosphere_request_maker, poisson_stream
+    reqs = poisson_stream(a.serve_requests, 40.0, atmosphere_request_maker(), seed=777 + 1000 * ctx.rank)
+    free, _ = torch.cuda.mem_get_info()
+    arena = min(int(free * 0.5), 32 << 30)
+    b = Batch(2, precision=PREC_MIXED, arena_bytes=arena, max_sims=256, device=ctx.local)
+    ctx.barrier()
+    st = Server(b, chunk=10, keep_results=False).run(reqs)
+    b.close()
+    st.update({"arrival_rate_per_s": 40.0, "chunk_steps": 10, "arena_bytes": arena,
+               "workload": "Poisson arrivals 40/s (seed 777) of driven atmosphere x-z slices "
+                           "{128x256, 256x512, 384x768, 512x1024}, period U[120,600] s, amplitude U[50,500] m/s, "
+                           "U[200,2000] steps, mixed precision; time to solution = arrival to result on the host"})
+    return st
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -450,6 +473,8 @@ def main():
     ap.add_argument("--no-blast", action="store_true", help="skip the 3-D blast wave measurements")
     ap.add_argument("--only-batched", action="store_true", help="just the timed batched run (profiling)")
     ap.add_argument("--ensemble-count", type=int, default=ENSEMBLE["count"])
+    ap.add_argument("--serve-requests", type=int, default=48,
+                    help="requests of the serving stream (0: skip); the full stream is 2000")
     ap.add_argument("--accuracy-steps", type=int, default=50,
                     help="steps of the blast-wave accuracy study against the FP64 oracle build (0: skip)")
     a = ap.parse_args()
@@ -475,6 +500,8 @@ def main():
         e2e = run_e2e_batched(probs, PREC_MIXED, ctx, K)
         if not a.no_blast:
             line_extra["blast128"] = run_blast(a, ctx)
+        if a.serve_requests > 0:
+            line_extra["serving"] = run_serving(a, ctx)
     else:
         e2e = None
 

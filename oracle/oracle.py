@@ -34,15 +34,20 @@ def build_oracle(force: bool = False) -> Path:
     return LIB
 
 
+class _Driver(ctypes.Structure):
+    _fields_ = [("on", _I), ("dir", _I), ("amp", _D), ("period", _D), ("center", _D * 3),
+                ("width", _D * 3), ("xmin", _D * 3), ("dx", _D * 3)]
+
+
 class _Grid(ctypes.Structure):
     _fields_ = [("ndim", _I), ("n", _I * 3), ("gamma", _D), ("chyp", _D * 13),
                 ("btype", _I * 3), ("g", _D * 3), ("courant", _D), ("hyperdif", _I),
-                ("delx", _PD * 3)]
+                ("delx", _PD * 3), ("drv", ctypes.POINTER(_Driver))]
 
 
 class _State(ctypes.Structure):
     _fields_ = [("dt", _D), ("dtdiffvisc", _D), ("maxviscoef", _D), ("maxcourant", _D),
-                ("cmax", _D * 3)]
+                ("cmax", _D * 3), ("t", _D)]
 
 
 def _ptr(a: np.ndarray):
@@ -78,6 +83,19 @@ class Oracle:
             g.chyp[f] = prob.chyp[f]
         g.courant = prob.courant
         g.hyperdif = prob.hyperdif
+        drv = getattr(prob, "driver", None)
+        self.drv = _Driver()
+        if drv:
+            self.drv.on = 1
+            self.drv.dir = int(drv.get("dir", 0))
+            self.drv.amp = float(drv["amp"])
+            self.drv.period = float(drv.get("period", 0.0))
+            for d in range(prob.ndim):
+                self.drv.center[d] = float(drv["center"][d])
+                self.drv.width[d] = float(drv["width"][d])
+                self.drv.xmin[d] = float(prob.xmin[d])
+                self.drv.dx[d] = float(prob.dx[d])
+            g.drv = ctypes.pointer(self.drv)
         self.g = g
         self.s = _State()
         self.s.dt = 1.0e-8 if dt_fixed == 0.0 else dt_fixed
@@ -118,6 +136,10 @@ class Oracle:
     def dt(self):
         return self.s.dt
 
+    @property
+    def t(self):
+        return self.s.t
+
 
 class Reference:
     """The reference's own step, built for the host (oracle/_ref).
@@ -127,8 +149,9 @@ class Reference:
 
     _loaded: dict = {}
 
-    def __init__(self, prob):
-        path = REF_DIR / f"libsmaug_ref{prob.ndim}d.so"
+    def __init__(self, prob, variant: str = ""):
+        """variant "drv": the 2-D build with the spicule model's driver."""
+        path = REF_DIR / f"libsmaug_ref{prob.ndim}d{'_' + variant if variant else ''}.so"
         if not path.exists():
             raise FileNotFoundError(f"{path} missing: run oracle/ref_shim/build_ref.py")
         L = ctypes.CDLL(str(path))

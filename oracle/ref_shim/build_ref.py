@@ -1,8 +1,9 @@
 #!/usr/bin/env python3
 """Host build of the SMAUG reference's own CUDA sources -- test infrastructure.
 
-Builds ``oracle/_ref/libsmaug_ref2d.so`` and ``oracle/_ref/libsmaug_ref3d.so``
-from the reference's unmodified-on-disk sources under
+Builds ``oracle/_ref/libsmaug_ref2d.so``, ``oracle/_ref/libsmaug_ref3d.so`` and
+``oracle/_ref/libsmaug_ref2d_drv.so`` (2-D with the spicule model's momentum
+driver) from the reference's unmodified-on-disk sources under
 ``<reference>/dev/smaug/src`` (read-only), so that the reference itself pins the
 oracle and the GPU path.  Nothing is copied into the repository: every
 generated file lands in ``oracle/_ref/`` (git-ignored, shipped with the other
@@ -180,11 +181,20 @@ TEMPLATE_FILES = {
     3: {"usersource.cu": "../models/usersource.cu.default", "init_user.cu": "../models/init_user.cu.sedov3d"},
 }
 
+# Library variants: name -> (ndim, model files replacing TEMPLATE_FILES, extra
+# defines).  "2d_drv" is the 2-D build with the spicule model's momentum
+# driver (models/usersource.cu.spicule1, compiled in by USE_USERSOURCE).
+VARIANTS = {
+    "2d": (2, {}, []),
+    "3d": (3, {}, []),
+    "2d_drv": (2, {"usersource.cu": "../models/usersource.cu.spicule1"}, ["-DUSE_USERSOURCE"]),
+}
+
 
 SOURCE_FILES = {"boundary.cu": "../models/boundary.cu.sedov3d"}
 
 
-def generate(ref_src: Path, build: Path, ndim: int) -> list[Path]:
+def generate(ref_src: Path, build: Path, ndim: int, models: dict | None = None) -> list[Path]:
     (build / "src").mkdir(parents=True, exist_ok=True)
     (build / "include").mkdir(parents=True, exist_ok=True)
     done = set()
@@ -195,7 +205,8 @@ def generate(ref_src: Path, build: Path, ndim: int) -> list[Path]:
             dst = build / "include" / f"{stem}_{modid}.cuh"
             if dst in done:
                 continue
-            src_file = ref_src / TEMPLATE_FILES[ndim].get(tmpl, tmpl)
+            files = dict(TEMPLATE_FILES[ndim], **(models or {}))
+            src_file = ref_src / files.get(tmpl, tmpl)
             body = add_missing_returns(src_file.read_text(errors="replace").replace("MODID", modid))
             dst.write_text(body)
             done.add(dst)
@@ -214,17 +225,18 @@ def compile_one(args):
     return obj
 
 
-def build(reference: Path, dims=(2, 3), jobs: int = 8) -> None:
+def build(reference: Path, variants=("2d", "3d", "2d_drv"), jobs: int = 8) -> None:
     ref_src = reference / "dev" / "smaug" / "src"
     if not ref_src.is_dir():
         raise FileNotFoundError(f"reference sources not found: {ref_src}")
     shim = HERE / "cuda_host_shim.h"
     driver = HERE / "ref_driver.cpp"
     OUT.mkdir(parents=True, exist_ok=True)
-    for d in dims:
-        build_dir = OUT / f"build{d}d"
-        srcs = generate(ref_src, build_dir, d)
-        defs = ["-DUSE_SAC"] if d == 2 else ["-DUSE_SAC_3D"]
+    for v in variants:
+        d, models, extra = VARIANTS[v]
+        build_dir = OUT / f"build{v}"
+        srcs = generate(ref_src, build_dir, d, models)
+        defs = (["-DUSE_SAC"] if d == 2 else ["-DUSE_SAC_3D"]) + extra
         base = ["g++", "-x", "c++", "-std=c++14", "-O2", "-ffp-contract=off", "-fPIC",
                 "-fno-strict-aliasing", "-w", "-include", str(shim),
                 "-I", str(ref_src), "-I", str(HERE)] + defs + EXTRA_FLAGS
@@ -236,7 +248,7 @@ def build(reference: Path, dims=(2, 3), jobs: int = 8) -> None:
             objs.append(obj)
         with cf.ThreadPoolExecutor(max_workers=jobs) as ex:
             list(ex.map(compile_one, jobs_list))
-        lib = OUT / f"libsmaug_ref{d}d.so"
+        lib = OUT / f"libsmaug_ref{v}.so"
         cmd = ["g++", "-shared", "-o", str(lib)] + [str(o) for o in objs] + ["-lm"] + EXTRA_FLAGS
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
@@ -248,9 +260,9 @@ def main() -> int:
     ap = argparse.ArgumentParser()
     ap.add_argument("--reference", default=os.environ.get("SMAUG_REFERENCE", "/root/reference"))
     ap.add_argument("--jobs", type=int, default=os.cpu_count() or 4)
-    ap.add_argument("--dims", default="2,3")
+    ap.add_argument("--variants", default=",".join(VARIANTS))
     a = ap.parse_args()
-    build(Path(a.reference), tuple(int(x) for x in a.dims.split(",")), a.jobs)
+    build(Path(a.reference), tuple(a.variants.split(",")), a.jobs)
     return 0
 
 

@@ -373,8 +373,41 @@ void sm_oracle_boundary(const sm_oracle_grid *g, double *w) {
 
 /* ------------------------------------------------------------- the stage */
 
+/* Driver (usersource.cu.spicule1:4-137) on every cell of wout; the ghost
+ * fill that follows overwrites the ghosts, as cuboundary does after cusource
+ * (iosmaug.cpp:1153-1166). */
+static void add_driver(const sm_oracle_grid *g, const lay_t *L, double *wout, double h, double t) {
+  const sm_oracle_driver *dv = g->drv;
+  if (!dv || !dv->on) return;
+  const int D = L->D;
+  double tdep = 1.0;
+  if (dv->period > 0.0) tdep = sin(2.0 * 3.14159265358979323846 * t / dv->period);
+  for (long idx = 0; idx < L->N; ++idx) {
+    int c[3];
+    coords(L, idx, c);
+    double f[3] = {1.0, 1.0, 1.0};
+    for (int d = 0; d < D; ++d) {
+      if (dv->width[d] > 0.0) {
+        const double x = (dv->xmin[d]) + (((double)c[d]) * (dv->dx[d]));
+        const double r2 = (x - dv->center[d]) * (x - dv->center[d]);
+        f[d] = exp(-r2 / (dv->width[d] * dv->width[d]));
+      }
+    }
+    double prod = f[1] * f[0];
+    if (D == 3) prod = prod * f[2];
+    const double vvz = dv->amp * prod * tdep;
+    double *m = F(wout, L->M0 + dv->dir);
+    m[idx] = m[idx] + h * vvz * (F(wout, L->RHO)[idx] + F(wout, L->RHOB)[idx]);
+  }
+}
+
 double sm_oracle_stage(const sm_oracle_grid *g, const double *win, const double *wbase, double *wout,
                        double h, const double *cmax) {
+  return sm_oracle_stage_t(g, win, wbase, wout, h, cmax, 0.0);
+}
+
+double sm_oracle_stage_t(const sm_oracle_grid *g, const double *win, const double *wbase, double *wout,
+                         double h, const double *cmax, double tin) {
   lay_t L0 = mklay(g);
   const lay_t *L = &L0;
   const long N = L->N;
@@ -580,6 +613,7 @@ double sm_oracle_stage(const sm_oracle_grid *g, const double *win, const double 
       }
   }
 
+  add_driver(g, L, wout, h, tin);
   sm_oracle_boundary(g, wout);
   free(pt);
   free(ptb);
@@ -610,7 +644,7 @@ int sm_oracle_step(const sm_oracle_grid *g, double *w, int step, int rk4, int dt
     double *w1 = work;
     sm_oracle_cmax(g, w, cm);
     for (int d = 0; d < L->D; ++d) s->cmax[d] = cm[d];
-    v = sm_oracle_stage(g, w, w, w1, dt, cm);
+    v = sm_oracle_stage_t(g, w, w, w1, dt, cm, s->t);
     numax = v;
     memcpy(w, w1, sizeof(double) * NV);
   } else {
@@ -618,17 +652,17 @@ int sm_oracle_step(const sm_oracle_grid *g, double *w, int step, int rk4, int dt
     double *w1 = work, *w2 = work + NV, *w3 = work + 2 * NV;
     sm_oracle_cmax(g, w, cm);
     for (int d = 0; d < L->D; ++d) s->cmax[d] = cm[d];
-    v = sm_oracle_stage(g, w, w, w1, dt / 2, cm); /* w1 = w + dt/2 k1 */
+    v = sm_oracle_stage_t(g, w, w, w1, dt / 2, cm, s->t + 0.0 * dt); /* w1 = w + dt/2 k1 */
     if (v > numax) numax = v;
     sm_oracle_cmax(g, w1, cm);
-    v = sm_oracle_stage(g, w1, w, w2, dt / 2, cm); /* w2 = w + dt/2 k2 */
+    v = sm_oracle_stage_t(g, w1, w, w2, dt / 2, cm, s->t + 0.5 * dt); /* w2 = w + dt/2 k2 */
     if (v > numax) numax = v;
     sm_oracle_cmax(g, w2, cm);
-    v = sm_oracle_stage(g, w2, w, w3, dt, cm); /* w3 = w + dt k3 */
+    v = sm_oracle_stage_t(g, w2, w, w3, dt, cm, s->t + 0.5 * dt); /* w3 = w + dt k3 */
     if (v > numax) numax = v;
     for (long i = 0; i < NW; ++i) w1[i] = (w1[i] + 2 * w2[i] + w3[i] - 4 * w[i]) / 3;
     sm_oracle_cmax(g, w3, cm);
-    v = sm_oracle_stage(g, w3, w, w2, dt / 6, cm); /* w + dt/6 k4 */
+    v = sm_oracle_stage_t(g, w3, w, w2, dt / 6, cm, s->t + 1.0 * dt); /* w + dt/6 k4 */
     if (v > numax) numax = v;
     for (long i = 0; i < NW; ++i) w[i] = w2[i] + w1[i];
     sm_oracle_boundary(g, w);
@@ -639,5 +673,6 @@ int sm_oracle_step(const sm_oracle_grid *g, double *w, int step, int rk4, int dt
    * host copy, restoring the previous value: the coefficient is a running
    * maximum over all steps. */
   if (numax > s->maxviscoef) s->maxviscoef = numax;
+  s->t += dt;
   return 0;
 }

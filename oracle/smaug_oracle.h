@@ -20,6 +20,26 @@
 extern "C" {
 #endif
 
+/*
+ * Momentum driver: the reference's user source term (addsourceterms2,
+ * models/usersource.cu.spicule1:4-137, applied by cusource after the other
+ * terms of a step, iosmaug.cpp:1153).  At every cell of the updated state:
+ *   m_dir += h * vvz * (rho + rhob),  vvz = amp * F * tdep,
+ *   F = f1 * f0 (2-D) or (f1 * f0) * f2 (3-D),
+ *   f_d = exp(-(x_d - center_d)^2 / (width_d * width_d)), 1 where width_d = 0,
+ *   x_d = xmin_d + i_d * dx_d,
+ *   tdep = sin(2 pi t / period) (the model's commented time dependence), or 1
+ *   when period = 0 (the model's choice).
+ * The reference model applies it on the first iteration only (p->it == 1); a
+ * run of one step compares like for like.
+ */
+typedef struct {
+  int on;
+  int dir;
+  double amp, period;
+  double center[3], width[3], xmin[3], dx[3];
+} sm_oracle_driver;
+
 typedef struct {
   int ndim;            /* 2 or 3 */
   int n[3];            /* cells per dim incl. ghosts (n[2] = 1 in 2-D) */
@@ -30,6 +50,7 @@ typedef struct {
   double courant;
   int hyperdif;        /* 1: hyperdiffusion sources on (p->hyperdifmom) */
   const double *delx[3];
+  const sm_oracle_driver *drv;  /* NULL: no driver */
 } sm_oracle_grid;
 
 /* Per-run scalars carried between steps (p->dt, p->dtdiffvisc, p->maxviscoef). */
@@ -39,6 +60,7 @@ typedef struct {
   double maxviscoef;
   double maxcourant;
   double cmax[3];
+  double t;            /* simulation time at the start of the next step */
 } sm_oracle_state;
 
 int sm_oracle_nvar(int ndim);
@@ -65,6 +87,9 @@ double sm_oracle_select_dt(const sm_oracle_grid *g, const double *w, int step, s
  */
 double sm_oracle_stage(const sm_oracle_grid *g, const double *win, const double *wbase,
                        double *wout, double h, const double *cmax);
+/* The same stage with the driver (if any) evaluated at time tin. */
+double sm_oracle_stage_t(const sm_oracle_grid *g, const double *win, const double *wbase,
+                         double *wout, double h, const double *cmax, double tin);
 
 /* Ghost fill of the evolved fields (models/boundary.cu.sedov3d semantics). */
 void sm_oracle_boundary(const sm_oracle_grid *g, double *w);
@@ -74,6 +99,8 @@ void sm_oracle_boundary(const sm_oracle_grid *g, double *w);
  * classical four-step Runge-Kutta (dev/sac/src/vac.t:447-462) around the
  * same operator.  dt_mode = 1 selects dt as the reference does, 0 keeps s->dt.
  * work must hold 4 * NVAR * N doubles.  step is the 1-based step index.
+ * The driver's stage times are t, t + dt/2, t + dt/2, t + dt (RK4) or t;
+ * s->t advances by dt.
  */
 int sm_oracle_step(const sm_oracle_grid *g, double *w, int step, int rk4, int dt_mode,
                    sm_oracle_state *s, double *work);

@@ -163,6 +163,121 @@ def orszag_tang(nx: int = 256, ny: int | None = None, b0_scale: float = 1.0,
                                  "seed": seed})
 
 
+# Stratified solar atmosphere (SI units; B in units where the magnetic
+# pressure is B^2/2, i.e. tesla / sqrt(mu0), as dervfields.cu:119-120 use it).
+R_GAS = 8.31e3           # J / (kg K), mu = 1 (initialisation_user.h.spicule1_mpi:378)
+G_SUN = -274.0           # m / s^2 along the vertical (dim 0)
+MU0 = 4.0e-7 * np.pi
+
+
+def temperature_profile(z, t_ch=6.0e3, t_co=1.0e6, z_tr=2.0e6, w_tr=0.2e6):
+    """T(z) = T_ch + (T_co - T_ch) (1 + tanh((z - z_tr) / w_tr)) / 2."""
+    return t_ch + (t_co - t_ch) * (1.0 + np.tanh((z - z_tr) / w_tr)) / 2.0
+
+
+def hydrostatic_density(z, T, rho0, g=G_SUN, R=R_GAS):
+    """rho_b(z) of an ideal gas (p = rho R T) in hydrostatic equilibrium,
+    dp/dz = rho g, with rho = rho0 at z = 0: p = p0 exp(-int_0^z dz'/lambda),
+    lambda = -R T / g, the integral by the trapezoid rule on the grid points z
+    (FP64), from the grid point at z = 0 outwards in both directions."""
+    inv = 1.0 / (-R * T / g)
+    i0 = int(np.argmin(np.abs(z)))
+    if z[i0] != 0.0:
+        raise ValueError("the grid needs a point at z = 0")
+    integ = np.zeros_like(z)
+    for i in range(i0 + 1, len(z)):
+        integ[i] = integ[i - 1] + 0.5 * (inv[i - 1] + inv[i]) * (z[i] - z[i - 1])
+    for i in range(i0 - 1, -1, -1):
+        integ[i] = integ[i + 1] - 0.5 * (inv[i + 1] + inv[i]) * (z[i + 1] - z[i])
+    p0 = rho0 * R * T[i0]
+    p = p0 * np.exp(-integ)
+    return p / (R * T), p
+
+
+def atmosphere(nz: int = 256, nx: int = 128, ny: int | None = None, lz: float = 6.0e6, lx: float = 4.0e6,
+               ly: float = 4.0e6, rho0: float = 2.7e-4, b_gauss: float = 10.0, gamma: float = 5.0 / 3.0,
+               driver: dict | None = "default", noise: float = 0.0, seed: int | None = None) -> Problem:
+    """Stratified solar atmosphere, vertical = dim 0 (z from 0 at the first
+    inner cell), 2-D (z, x) when ny is None, else 3-D (z, x, y).  Split
+    background: T(z) tanh profile, rho_b hydrostatic, p_b = rho_b R T, uniform
+    vertical B_b, e_b = p_b / (gamma - 1) + B_b^2 / 2; perturbations zero (or
+    seeded density noise of relative size `noise`).  Vertical boundaries
+    contcd4, lateral periodic, gravity along -z.  driver "default": vertical
+    velocity driver at the lower boundary, 300 s period, 200 m/s, 0.5 Mm
+    horizontal width."""
+    D = 2 if ny is None else 3
+    cells = (nz, nx) if D == 2 else (nz, nx, ny)
+    L = (lz, lx) if D == 2 else (lz, lx, ly)
+    n = tuple(c + 2 * NG for c in cells)
+    dx = tuple(L[d] / cells[d] for d in range(D))
+    xmin = tuple(-NG * dx[d] for d in range(D))
+    z = xmin[0] + np.arange(n[0]) * dx[0]
+    T = temperature_profile(z)
+    rhob, pb = hydrostatic_density(z, T, rho0)
+    bz = b_gauss * 1.0e-4 / np.sqrt(MU0)
+    ids = field_ids(D)
+    shape = tuple(reversed(n))  # arrays are indexed [.., dim1, dim0]
+    w = np.zeros((nvar(D),) + shape)
+    prof = lambda a: np.broadcast_to(a, shape)  # noqa: E731  (dim 0 is the last axis)
+    w[ids["rhob"]] = prof(rhob)
+    w[ids["b1b"]] = bz
+    w[ids["eb"]] = prof(pb / (gamma - 1.0) + 0.5 * bz * bz)
+    if noise:
+        rng = np.random.default_rng(seed)
+        w[ids["rho"]] = noise * prof(rhob) * rng.standard_normal(shape)
+    drv = None
+    if driver == "default":
+        drv = {"dir": 0, "amp": 200.0, "period": 300.0,
+               "center": (2.0 * dx[0],) + tuple(L[d] / 2 for d in range(1, D)),
+               "width": (2.0 * dx[0],) + (0.5e6,) * (D - 1)}
+    elif driver:
+        drv = dict(driver)
+    prob = Problem("atmosphere", D, n, dx, xmin, gamma, _chyp(D), (4,) + (0,) * (D - 1), 0.3, w,
+                   g=(G_SUN, 0.0, 0.0), meta={"nz": nz, "nx": nx, "ny": ny, "noise": noise, "seed": seed},
+                   driver=drv)
+    if noise:
+        prob.w = _boundary_fill(prob)
+    return prob
+
+
+def _boundary_fill(prob: Problem) -> np.ndarray:
+    """Ghost fill of the evolved fields: periodic or contcd4 per dim (the
+    state handed to the library gets this fill again on load)."""
+    w = prob.w.copy()
+    nw = 2 + 2 * prob.ndim
+    for d in range(prob.ndim):
+        ax = w.ndim - 1 - d
+        m = w.shape[ax]
+        idx = np.arange(m)
+        if prob.btype[d] == 0:
+            src = np.where(idx < NG, idx + m - 2 * NG, np.where(idx >= m - NG, idx - (m - 2 * NG), idx))
+        else:  # contcd4: 0 <- 4, 1 <- 3, n-1 <- n-5, n-2 <- n-4
+            src = idx.copy()
+            src[0], src[1], src[m - 1], src[m - 2] = 4, 3, m - 5, m - 4
+        w[:nw] = np.take(w[:nw], src, axis=ax)
+    return w
+
+
+def driver_slab(n: int = 24) -> Problem:
+    """2-D (z, x) uniform slab in metres around the driver of the reference's
+    spicule model (models/usersource.cu.spicule1: centre z = 0.0174 Mm,
+    x = 1.998046 Mm, widths 1 km, 200 m/s, constant in time), 250 m cells, so
+    that its Gaussian spans several cells.  rho = 1e-3, p = 1e3, B = (1e-2, 0)."""
+    D = 2
+    N = (n + 2 * NG,) * 2
+    dx = (250.0, 250.0)
+    c = (0.0174e6, 1.998046e6)
+    xmin = tuple(c[d] - (N[d] // 2) * dx[d] + 0.3 * dx[d] for d in range(D))
+    gam = 5.0 / 3.0
+    ids = field_ids(D)
+    w = np.zeros((nvar(D),) + tuple(reversed(N)))
+    w[ids["rho"]] = 1.0e-3
+    w[ids["b1"]] = 1.0e-2
+    w[ids["e"]] = 1.0e3 / (gam - 1.0) + 0.5 * 1.0e-4
+    drv = {"dir": 0, "amp": 200.0, "period": 0.0, "center": c, "width": (1.0e3, 1.0e3)}
+    return Problem("driver_slab", D, N, dx, xmin, gam, _chyp(D), (0, 0), 0.3, w, driver=drv)
+
+
 ENSEMBLE_SIDES = (128, 192, 256, 384, 512, 768)
 
 

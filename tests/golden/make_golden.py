@@ -35,13 +35,55 @@ CASES = {
     "blast10_cd4x_euler": dict(kind="blast", n=10, btype=[4, 0, 0], steps=3, rk4=False),
     "ot24_rk4": dict(kind="ot", n=24, btype=None, steps=4, rk4=True),
     "blast10_rk4": dict(kind="blast", n=10, btype=None, steps=3, rk4=True),
+    # the reference built with its spicule model's momentum driver; the model
+    # drives on the first iteration only, so one step
+    "slab24_driver_euler": dict(kind="slab", n=24, btype=None, steps=1, rk4=False, variant="drv"),
+    # stratified atmosphere slice: gravity, contcd4 vertical boundaries,
+    # non-zero background fields, seeded density perturbation
+    "atmos40x20_euler": dict(kind="atmos", n=[40, 20], btype=None, steps=4, rk4=False),
+    "atmos40x20_drv_rk4": dict(kind="atmos", n=[40, 20], btype=None, steps=3, rk4=True, driver="const"),
 }
+
+
+def quirk_mask(spec, shape, source):
+    """Cells excluded from a comparison with a fixture made by the reference.
+
+    The reference's contcd4 boundary kernel for dim 0
+    (models/boundary.cu.sedov3d:16-80) has no bound on the row index, so the
+    threads beyond the grid write one row past the field they fill.  Fields
+    0..NW-2 overwrite the spill in their own pass later; the pass of the last
+    evolved field spills into the first background field, eb, at the two
+    corner ghost cells (0,0) and (1,0) in 2-D (iindex -> j = nj).  No stencil
+    of an inner cell reads them; the library never writes background fields,
+    so these two cells keep their input values there."""
+    mask = np.ones(shape, dtype=bool)
+    btype = spec.get("btype") or ([4] + [0] * (len(shape) - 2) if spec["kind"] == "atmos" else None)
+    if source == "reference" and len(shape) == 3 and btype and btype[0] == 4:
+        nw = 6
+        flat = mask[nw].reshape(-1)
+        flat[0:2] = False
+    return mask
+
+
+def states_match(w, gold_w, spec, source):
+    """Bit-exact equality outside the quirk cells."""
+    m = quirk_mask(spec, gold_w.shape, source)
+    return bool(np.array_equal(w[m], gold_w[m]))
 
 
 def make_problem(spec):
     from smaug_b200 import problems
     if spec["kind"] == "ot":
         prob = problems.orszag_tang(spec["n"])
+    elif spec["kind"] == "slab":
+        prob = problems.driver_slab(spec["n"])
+    elif spec["kind"] == "atmos":
+        prob = problems.atmosphere(spec["n"][0], spec["n"][1], noise=1e-3, seed=3, driver=None)
+        if spec.get("driver") == "const":  # the default driver, constant in time (tdep = 1)
+            d = problems.atmosphere(spec["n"][0], spec["n"][1]).driver
+            d["period"] = 0.0
+            d["amp"] = 2.0e3
+            prob.driver = d
     else:
         prob = problems.blast_wave(spec["n"])
     if spec.get("btype"):
@@ -62,7 +104,7 @@ def run_case(name: str) -> None:
         states.append(o.w.copy())
         source = "oracle"
     else:
-        r = Reference(prob)
+        r = Reference(prob, variant=spec.get("variant", ""))
         for _ in range(spec["steps"]):
             w = r.step(1)
             dts.append(r.dt)

@@ -98,3 +98,19 @@ def test_batch_fixed_dt_and_dt_rule_mixed(need_gpu):
     assert np.array_equal(b.state(s1), alone(p1, 4, PREC_FP64, dt_mode=0, dt0=1e-3)[0])
     assert np.array_equal(b.state(s2), alone(p2, 4, PREC_FP64)[0])
     assert b.scalars(s1)["dt"] == 1e-3
+
+
+def test_batch_atmosphere_slices_with_driver(need_gpu):
+    """Driven atmosphere slices of different sizes and driver periods in one
+    batch give the bits they give alone (the driver clock is per simulation)."""
+    probs = [problems.atmosphere(40, 20, noise=1e-3, seed=1), problems.atmosphere(64, 32, noise=1e-3, seed=2),
+             problems.atmosphere(48, 16, noise=1e-3, seed=3)]
+    for k, p in enumerate(probs):
+        p.driver["amp"] = 1.0e3 * (k + 1)
+        p.driver["period"] = 2.0 + k
+    steps = [5, 7, 3]
+    b = Batch(2, precision=PREC_MIXED, arena_bytes=128 << 20, max_sims=4)
+    slots = [b.add(p, k) for p, k in zip(probs, steps)]
+    b.step(8)
+    for p, k, s in zip(probs, steps, slots):
+        assert np.array_equal(b.state(s), alone(p, k, PREC_MIXED)[0])
