@@ -1,0 +1,5 @@
+// Stage kernels of the batch for ndim 2, float stencils (batch_kernels.inc).
+#define BATCH_D 2
+#define BATCH_T float
+#define BATCH_SUFFIX f
+#include "batch_kernels.inc"

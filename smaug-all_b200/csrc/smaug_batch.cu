@@ -259,6 +259,7 @@ int smaug_batch_create(int ndim, int precision, int device, size_t arena_bytes, 
   if (arena_bytes < 4096) return bfail(b, SMAUG_ERR_ARG, "arena too small");
   b->D = ndim;
   b->mixed = precision == SMAUG_PREC_MIXED;
+  b->variant = batch_default_variant(ndim, b->mixed);
   b->device = device;
   b->max_inst = max_sims;
   b->arena_bytes = arena_bytes & ~(size_t)255;

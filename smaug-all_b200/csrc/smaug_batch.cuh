@@ -24,35 +24,82 @@ struct WorkItem {
   int tile;
 };
 
-// Tile shapes the batch kernels are built for (the autotuner picks one).
-constexpr int kBatchVariants2 = 4;  // 2-D: 16x16, 32x8, 8x32, 32x16
-constexpr int kBatchVariants3 = 3;  // 3-D: 8x8x4, 16x8x2, 32x4x2
-__host__ __device__ inline void batch_tile_shape(int D, int v, int *t) {
-  t[2] = 1;
+// Tile shapes and occupancy targets (resident blocks per SM the register
+// allocation is made for) the stage kernel is built for; the autotuner picks
+// one.  Variant 0 is the single-simulation default.
+constexpr int kBatchVariants2 = 10;
+constexpr int kBatchVariants3 = 6;
+struct BatchVariant {
+  int t[3];
+  int min_blocks;
+};
+__host__ __device__ inline BatchVariant batch_variant(int D, int v) {
   if (D == 2) {
     switch (v) {
-      case 1: t[0] = 32; t[1] = 8; break;
-      case 2: t[0] = 8; t[1] = 32; break;
-      case 3: t[0] = 32; t[1] = 16; break;
-      default: t[0] = 16; t[1] = 16; break;
-    }
-  } else {
-    switch (v) {
-      case 1: t[0] = 16; t[1] = 8; t[2] = 2; break;
-      case 2: t[0] = 32; t[1] = 4; t[2] = 2; break;
-      default: t[0] = 8; t[1] = 8; t[2] = 4; break;
+      case 1: return {{32, 8, 1}, 2};
+      case 2: return {{8, 32, 1}, 2};
+      case 3: return {{32, 16, 1}, 1};
+      case 4: return {{16, 16, 1}, 3};
+      case 5: return {{32, 8, 1}, 3};
+      case 6: return {{16, 16, 1}, 4};
+      case 7: return {{32, 8, 1}, 4};
+      case 8: return {{16, 16, 1}, 5};
+      case 9: return {{16, 8, 1}, 8};
+      default: return {{16, 16, 1}, 2};
     }
   }
+  switch (v) {
+    case 1: return {{16, 8, 2}, 2};
+    case 2: return {{32, 4, 2}, 2};
+    case 3: return {{8, 8, 4}, 3};
+    case 4: return {{16, 8, 2}, 3};
+    case 5: return {{8, 8, 4}, 4};
+    default: return {{8, 8, 4}, 2};
+  }
+}
+
+// Default variant of a single simulation and of an untuned batch, per ndim
+// and precision (the fastest of the variants in a B200 sweep of RK stage 1:
+// 96 Orszag-Tang simulations 128^2..768^2, one 128^3 blast wave).  A batch
+// and a single-simulation context on the same variant give the same bits.
+__host__ __device__ inline int batch_default_variant(int D, bool mixed) {
+  if (D == 2) return mixed ? 8 : 4;
+  return mixed ? 3 : 0;
+}
+
+__host__ __device__ inline void batch_tile_shape(int D, int v, int *t) {
+  const BatchVariant b = batch_variant(D, v);
+  t[0] = b.t[0];
+  t[1] = b.t[1];
+  t[2] = b.t[2];
 }
 
 }  // namespace smaug
 
 namespace smaug_batchk {
+// per (ndim, stencil type) translation units (batch_k{2,3}{f,d}.cu)
+void launch_batch_stage_2f(int, const smaug::BatchInst *, const smaug::WorkItem *, int, int, int, cudaStream_t);
+void launch_batch_stage_2d(int, const smaug::BatchInst *, const smaug::WorkItem *, int, int, int, cudaStream_t);
+void launch_batch_stage_3f(int, const smaug::BatchInst *, const smaug::WorkItem *, int, int, int, cudaStream_t);
+void launch_batch_stage_3d(int, const smaug::BatchInst *, const smaug::WorkItem *, int, int, int, cudaStream_t);
+int batch_stage_occupancy_2f(int);
+int batch_stage_occupancy_2d(int);
+int batch_stage_occupancy_3f(int);
+int batch_stage_occupancy_3d(int);
+
 // Launch one RK stage (1..4) for every work item whose simulation takes the
 // current step (work == nullptr: items are the tiles of simulation 0).
 // grid: persistent block count.
-void launch_batch_stage(int D, bool mixed, int variant, const smaug::BatchInst *tab, const smaug::WorkItem *work,
-                        int nwork, int stage, int grid, cudaStream_t st);
+inline void launch_batch_stage(int D, bool mixed, int variant, const smaug::BatchInst *tab,
+                               const smaug::WorkItem *work, int nwork, int stage, int grid, cudaStream_t st) {
+  if (D == 2)
+    (mixed ? launch_batch_stage_2f : launch_batch_stage_2d)(variant, tab, work, nwork, stage, grid, st);
+  else
+    (mixed ? launch_batch_stage_3f : launch_batch_stage_3d)(variant, tab, work, nwork, stage, grid, st);
+}
 // Blocks per SM the stage kernel of (D, mixed, variant) can keep resident.
-int batch_stage_occupancy(int D, bool mixed, int variant);
+inline int batch_stage_occupancy(int D, bool mixed, int variant) {
+  if (D == 2) return mixed ? batch_stage_occupancy_2f(variant) : batch_stage_occupancy_2d(variant);
+  return mixed ? batch_stage_occupancy_3f(variant) : batch_stage_occupancy_3d(variant);
+}
 }  // namespace smaug_batchk

@@ -101,7 +101,8 @@ void launch_stage(Run &r, const StageArgs &a) {
 // block per tile of this simulation.
 void launch_rk_stage(Run &r, int k) {
   timed_launch(r, [&] {
-    smaug_batchk::launch_batch_stage(r.D, r.mixed, 0, r.inst, nullptr, r.ntiles, k, r.ntiles, r.stream);
+    smaug_batchk::launch_batch_stage(r.D, r.mixed, batch_default_variant(r.D, r.mixed), r.inst, nullptr, r.ntiles, k,
+                                     r.ntiles, r.stream);
   });
 }
 
@@ -119,7 +120,7 @@ cudaError_t run_upload_inst(Run &r) {
   I.sc = r.sc;
   I.active = 1;
   int t[3];
-  batch_tile_shape(r.D, 0, t);
+  batch_tile_shape(r.D, batch_default_variant(r.D, r.mixed), t);
   r.ntiles = 1;
   for (int d = 0; d < 3; ++d) {
     I.tiles[d] = d < r.D ? (r.geo.n[d] - 4 + t[d] - 1) / t[d] : 1;

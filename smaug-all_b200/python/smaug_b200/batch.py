@@ -99,9 +99,9 @@ class Batch:
     def tune(self, reps: int = 5):
         """Autotune the tile shape; returns (chosen variant, ms per variant)."""
         v = ctypes.c_int(-1)
-        ms = (ctypes.c_double * 8)()
-        self._check(self.lib.smaug_batch_tune(self.h, reps, ctypes.byref(v), ms, 8), "smaug_batch_tune")
-        nv = 4 if self.ndim == 2 else 3
+        ms = (ctypes.c_double * 16)()
+        self._check(self.lib.smaug_batch_tune(self.h, reps, ctypes.byref(v), ms, 16), "smaug_batch_tune")
+        nv = 10 if self.ndim == 2 else 6
         return v.value, list(ms[:nv])
 
     def set_variant(self, v: int):

@@ -27,7 +27,10 @@ COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC,-O2", "--expt-r
 UNITS = [
     ("stage_exact.cu", ["-fmad=false"]),
     ("stage_fast.cu", ["-fmad=true", "-ftz=true"]),
-    ("batch_kernels.cu", ["-fmad=true", "-ftz=true"]),
+    ("batch_k2f.cu", ["-fmad=true", "-ftz=true"]),
+    ("batch_k2d.cu", ["-fmad=true", "-ftz=true"]),
+    ("batch_k3f.cu", ["-fmad=true", "-ftz=true"]),
+    ("batch_k3d.cu", ["-fmad=true", "-ftz=true"]),
     ("smaug_capi.cu", []),
     ("smaug_batch.cu", []),
 ]

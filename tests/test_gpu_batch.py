@@ -50,7 +50,7 @@ def test_batch_matches_single_simulation(need_gpu, precision):
 def test_batch_tile_shapes_and_graph_replay_are_identical(need_gpu):
     probs = ot_mix()[:3]
     ref = [alone(p, 21, PREC_MIXED)[0] for p in probs]
-    for v in range(4):
+    for v in range(10):
         b = Batch(2, precision=PREC_MIXED, arena_bytes=256 << 20, max_sims=4)
         slots = [b.add(p, 21) for p in probs]
         b.set_variant(v)
@@ -65,7 +65,7 @@ def test_batch_3d(need_gpu):
     b = Batch(3, precision=PREC_MIXED, arena_bytes=256 << 20, max_sims=4)
     slots = [b.add(p, 4) for p in probs]
     v, ms = b.tune(reps=2)
-    assert 0 <= v < 3 and all(m > 0 for m in ms)
+    assert 0 <= v < 6 and len(ms) == 6 and all(m > 0 for m in ms)
     b.step(4)
     for p, s in zip(probs, slots):
         assert np.array_equal(b.state(s), alone(p, 4, PREC_MIXED)[0])
