@@ -63,7 +63,7 @@ __host__ __device__ inline BatchVariant batch_variant(int D, int v) {
 // 96 Orszag-Tang simulations 128^2..768^2, one 128^3 blast wave).  A batch
 // and a single-simulation context on the same variant give the same bits.
 __host__ __device__ inline int batch_default_variant(int D, bool mixed) {
-  if (D == 2) return mixed ? 8 : 4;
+  if (D == 2) return mixed ? 8 : 0;
   return mixed ? 3 : 0;
 }
 

@@ -311,7 +311,9 @@ __global__ void __launch_bounds__(kBX *kBY) stage_kernel(StageArgs a, Geo g, Phy
     if (p.drv_on) {
       const double vvz = driver_vvz<D>(g, p, a.sc, a.tfrac, c);
       const double rb = __ldg(a.bg + (long long)(L::RHOB - NW) * N + idx);
-      o[L::M0 + p.drv_dir] = o[L::M0 + p.drv_dir] + h * vvz * (o[L::RHO] + rb);
+#pragma unroll
+      for (int k = 0; k < D; ++k)
+        if (k == p.drv_dir) o[L::M0 + k] = o[L::M0 + k] + h * vvz * (o[L::RHO] + rb);
     }
 
     // ---- Runge-Kutta combination (vac.t:447-462)

@@ -159,6 +159,119 @@ __device__ __forceinline__ void q_all(const CellT<D, T> &c, long long i, int d, 
     if (f != d) q[s++] = c.v(L::B0 + f, i);
 }
 
+// The end of a stage for one cell (all threads of the block call it; the
+// inactive ones only take part in the block's maxima): the stage output
+// base + h dL with the driver, the RK combination of the stage, the writes of
+// the cell and its ghost images, and the wave-speed / viscosity maxima.
+template <int D, typename T>
+__device__ __forceinline__ void stage_epilogue(const StageArgs &a, const Geo &g, const Phys &p, const CellT<D, T> &C,
+                                               const int *c, bool active, long long idx, double h, const T *dL,
+                                               T numax) {
+  using L = Lay<D>;
+  constexpr int NW = L::NW, NB = L::NVAR - NW;
+  constexpr bool MIXED = sizeof(T) == sizeof(float);
+  double red[6] = {0, 0, 0, 0, 0, (double)numax};
+  if (active) {
+    double o[NW];
+    float hi[NW], lo[NW];
+    if (!MIXED) {
+#pragma unroll
+      for (int f = 0; f < NW; ++f) o[f] = a.base[(long long)f * g.N + idx] + h * (double)dL[f];
+      if (p.drv_on) {  // momentum driver on the stage output (before the RK combination)
+        const double vvz = driver_vvz<D>(g, p, a.sc, a.tfrac, c);
+        const double rb = __ldg(a.bg + (long long)(L::RHOB - NW) * g.N + idx);
+        // (unrolled compare: a runtime index would push o to local memory)
+#pragma unroll
+        for (int k = 0; k < D; ++k)
+          if (k == p.drv_dir) o[L::M0 + k] = o[L::M0 + k] + h * vvz * (o[L::RHO] + rb);
+      }
+      if (a.kind == 3) {
+#pragma unroll
+        for (int f = 0; f < NW; ++f) {
+          const long long j = (long long)f * g.N + idx;
+          a.acc[j] = (a.acc[j] + 2.0 * C.vd(f, idx) + o[f] - 4.0 * a.base[j]) * (1.0 / 3.0);
+        }
+      } else if (a.kind == 4) {
+#pragma unroll
+        for (int f = 0; f < NW; ++f) o[f] += a.acc[(long long)f * g.N + idx];
+      }
+    } else {
+      // RK4 in increment form, W = w32 + c32:
+      //   stages k = 1..3: S_k = W + h_k L_k (FP32), A += c_k h_k L_k with
+      //   c = 1/3, 2/3, 1/3, so A = (S1 + 2 S2 + S3 - 4 W) / 3 as the FP64 path;
+      //   stage 4: W <- W + h_4 L_4 + A, kept as value + compensation.
+      // Stages 1..3 round to FP32 anyway, so they take the base without c32.
+      double incs[NW];
+#pragma unroll
+      for (int f = 0; f < NW; ++f) incs[f] = h * (double)dL[f];
+      if (p.drv_on) {  // momentum driver with the stage output's density
+        const double wr = a.kind == 4 ? (double)a.w32[idx] + (double)a.c32[idx] : (double)a.w32[idx];
+        const double rb = __ldg(a.bg + (long long)(L::RHOB - NW) * g.N + idx);
+        const double dm = h * driver_vvz<D>(g, p, a.sc, a.tfrac, c) * ((wr + incs[L::RHO]) + rb);
+#pragma unroll
+        for (int k = 0; k < D; ++k)
+          if (k == p.drv_dir) incs[L::M0 + k] += dm;
+      }
+#pragma unroll
+      for (int f = 0; f < NW; ++f) {
+        const long long j = (long long)f * g.N + idx;
+        const double inc = incs[f];
+        if (a.kind == 4) {
+          const double wn = ((double)a.w32[j] + (double)a.c32[j]) + (inc + (double)a.acc32[j]);
+          hi[f] = (float)wn;
+          lo[f] = (float)(wn - (double)hi[f]);
+        } else {
+          hi[f] = (float)((double)a.w32[j] + inc);
+          const double prev = a.kind == 1 ? 0.0 : (double)a.acc32[j];
+          a.acc32[j] = (float)(prev + (a.kind == 2 ? 2.0 : 1.0) * (1.0 / 3.0) * inc);
+        }
+        o[f] = (double)hi[f];  // what the next stage reads
+      }
+    }
+    // the cell and its ghost images: per dim the own coordinate and, at most,
+    // one image coordinate (images()), combined over all dims
+    int x0[3], x1[3], has[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      int xs[2] = {0, 0};
+      has[d] = d < D ? (images(g, d, c[d], xs) == 2) : 0;
+      x0[d] = d < D ? c[d] : 0;
+      x1[d] = xs[1];
+    }
+#pragma unroll
+    for (int m = 0; m < (1 << D); ++m) {
+      bool ok = true;
+      int cc[3];
+#pragma unroll
+      for (int d = 0; d < 3; ++d) {
+        const bool b = d < D && ((m >> d) & 1);
+        if (b && !has[d]) ok = false;
+        cc[d] = b ? x1[d] : x0[d];
+      }
+      if (!ok) continue;
+      const long long j = gidx<D>(g, cc);
+      if (!MIXED) {
+#pragma unroll
+        for (int f = 0; f < NW; ++f) a.out[(long long)f * g.N + j] = o[f];
+      } else if (a.kind == 4) {
+#pragma unroll
+        for (int f = 0; f < NW; ++f) {
+          a.w32[(long long)f * g.N + j] = hi[f];
+          a.c32[(long long)f * g.N + j] = lo[f];
+        }
+      } else {
+#pragma unroll
+        for (int f = 0; f < NW; ++f) a.out32[(long long)f * g.N + j] = hi[f];
+      }
+      double bgv[NB];
+#pragma unroll
+      for (int b = 0; b < NB; ++b) bgv[b] = __ldg(a.bg + (long long)b * g.N + j);
+      reduce_cell<D>(g, p, o, bgv, j, red);
+    }
+  }
+  block_max_flush<6>(red, &a.sc->red[a.red_out]);
+}
+
 // One RK stage on the tile (bx, by, bz) of one simulation; every thread of
 // the block calls it (it synchronises the block).  sm: tile_smem_elems<D, S>()
 // elements of T.
@@ -459,101 +572,7 @@ __device__ __forceinline__ void tile_body(const StageArgs &a, const Geo &g, cons
     __syncthreads();
   }
 
-  // ------------------------------------------------ combine, write, reduce
-  double red[6] = {0, 0, 0, 0, 0, (double)numax};
-  if (active) {
-    double o[NW];
-    float hi[NW], lo[NW];
-    if (!MIXED) {
-#pragma unroll
-      for (int f = 0; f < NW; ++f) o[f] = a.base[(long long)f * g.N + idx] + h * (double)dL[f];
-      if (p.drv_on) {  // momentum driver on the stage output (before the RK combination)
-        const double vvz = driver_vvz<D>(g, p, a.sc, a.tfrac, c);
-        const double rb = __ldg(a.bg + (long long)(L::RHOB - NW) * g.N + idx);
-        o[L::M0 + p.drv_dir] = o[L::M0 + p.drv_dir] + h * vvz * (o[L::RHO] + rb);
-      }
-      if (a.kind == 3) {
-#pragma unroll
-        for (int f = 0; f < NW; ++f) {
-          const long long j = (long long)f * g.N + idx;
-          a.acc[j] = (a.acc[j] + 2.0 * C.vd(f, idx) + o[f] - 4.0 * a.base[j]) * (1.0 / 3.0);
-        }
-      } else if (a.kind == 4) {
-#pragma unroll
-        for (int f = 0; f < NW; ++f) o[f] += a.acc[(long long)f * g.N + idx];
-      }
-    } else {
-      // RK4 in increment form, W = w32 + c32:
-      //   stages k = 1..3: S_k = W + h_k L_k (FP32), A += c_k h_k L_k with
-      //   c = 1/3, 2/3, 1/3, so A = (S1 + 2 S2 + S3 - 4 W) / 3 as the FP64 path;
-      //   stage 4: W <- W + h_4 L_4 + A, kept as value + compensation.
-      // Stages 1..3 round to FP32 anyway, so they take the base without c32.
-      double incs[NW];
-#pragma unroll
-      for (int f = 0; f < NW; ++f) incs[f] = h * (double)dL[f];
-      if (p.drv_on) {  // momentum driver with the stage output's density
-        const double wr = a.kind == 4 ? (double)a.w32[idx] + (double)a.c32[idx] : (double)a.w32[idx];
-        const double rb = __ldg(a.bg + (long long)(L::RHOB - NW) * g.N + idx);
-        incs[L::M0 + p.drv_dir] += h * driver_vvz<D>(g, p, a.sc, a.tfrac, c) * ((wr + incs[L::RHO]) + rb);
-      }
-#pragma unroll
-      for (int f = 0; f < NW; ++f) {
-        const long long j = (long long)f * g.N + idx;
-        const double inc = incs[f];
-        if (a.kind == 4) {
-          const double wn = ((double)a.w32[j] + (double)a.c32[j]) + (inc + (double)a.acc32[j]);
-          hi[f] = (float)wn;
-          lo[f] = (float)(wn - (double)hi[f]);
-        } else {
-          hi[f] = (float)((double)a.w32[j] + inc);
-          const double prev = a.kind == 1 ? 0.0 : (double)a.acc32[j];
-          a.acc32[j] = (float)(prev + (a.kind == 2 ? 2.0 : 1.0) * (1.0 / 3.0) * inc);
-        }
-        o[f] = (double)hi[f];  // what the next stage reads
-      }
-    }
-    // the cell and its ghost images: per dim the own coordinate and, at most,
-    // one image coordinate (images()), combined over all dims
-    int x0[3], x1[3], has[3];
-#pragma unroll
-    for (int d = 0; d < 3; ++d) {
-      int xs[2] = {0, 0};
-      has[d] = d < D ? (images(g, d, c[d], xs) == 2) : 0;
-      x0[d] = d < D ? c[d] : 0;
-      x1[d] = xs[1];
-    }
-#pragma unroll
-    for (int m = 0; m < (1 << D); ++m) {
-      bool ok = true;
-      int cc[3];
-#pragma unroll
-      for (int d = 0; d < 3; ++d) {
-        const bool b = d < D && ((m >> d) & 1);
-        if (b && !has[d]) ok = false;
-        cc[d] = b ? x1[d] : x0[d];
-      }
-      if (!ok) continue;
-      const long long j = gidx<D>(g, cc);
-      if (!MIXED) {
-#pragma unroll
-        for (int f = 0; f < NW; ++f) a.out[(long long)f * g.N + j] = o[f];
-      } else if (a.kind == 4) {
-#pragma unroll
-        for (int f = 0; f < NW; ++f) {
-          a.w32[(long long)f * g.N + j] = hi[f];
-          a.c32[(long long)f * g.N + j] = lo[f];
-        }
-      } else {
-#pragma unroll
-        for (int f = 0; f < NW; ++f) a.out32[(long long)f * g.N + j] = hi[f];
-      }
-      double bgv[NB];
-#pragma unroll
-      for (int b = 0; b < NB; ++b) bgv[b] = __ldg(a.bg + (long long)b * g.N + j);
-      reduce_cell<D>(g, p, o, bgv, j, red);
-    }
-  }
-  block_max_flush<6>(red, &a.sc->red[a.red_out]);
+  stage_epilogue<D, T>(a, g, p, C, c, active, idx, h, dL, numax);
 }
 
 // One launch = one RK stage of one simulation, one block per tile.
