@@ -245,6 +245,34 @@ void *smaug_batch_stream(smaug_batch *b);
 long long smaug_batch_launch_count(smaug_batch *b);
 const char *smaug_batch_last_error(smaug_batch *b);
 
+/*
+ * VAC configuration files: the reference's format for initial conditions and
+ * snapshots (host only).  ascii .ini as readasciivacconfig reads it
+ * (src/readwrite.c:982-1112); binary .out as writevacconfig writes it
+ * (src/readwrite.c:160-368).  Positions are ndim arrays of N doubles (the
+ * reference's wd[pos1..]), states nw arrays of N doubles (wmod slot layout),
+ * x fastest, N = n[0] * .. * n[ndim-1].  The readers fill the header; with pos
+ * and w both NULL they stop there (so a caller can size its buffers first).
+ * Errors return SMAUG_ERR_ARG with smaug_vac_last_error() (per thread).
+ */
+typedef struct {
+  char name[80];     /* first line / 79-byte name */
+  int it;            /* iteration number (state.it) */
+  double t;          /* simulation time (state.t) */
+  int ndim, neqpar, nw;
+  int n[3];          /* cells per dim (n[d] = 1 beyond ndim) */
+  double eqpar[16];  /* gamma, eta, g_1 .. g_ndim, ... (neqpar of them) */
+  char names[80];    /* variable names line */
+} smaug_vac_header;
+
+int smaug_vac_read_ascii(const char *path, smaug_vac_header *hdr, double *pos, size_t pos_count, double *w,
+                         size_t w_count);
+int smaug_vac_write_ascii(const char *path, const smaug_vac_header *hdr, const double *pos, const double *w);
+int smaug_vac_read_binary(const char *path, smaug_vac_header *hdr, double *pos, size_t pos_count, double *w,
+                          size_t w_count);
+int smaug_vac_write_binary(const char *path, const smaug_vac_header *hdr, const double *pos, const double *w);
+const char *smaug_vac_last_error(void);
+
 /* The CUDA stream (cudaStream_t) all work of ctx is ordered on. */
 void *smaug_stream(smaug_ctx *ctx);
 

@@ -33,12 +33,14 @@ UNITS = [
     ("batch_k3d.cu", ["-fmad=true", "-ftz=true"]),
     ("smaug_capi.cu", []),
     ("smaug_batch.cu", []),
+    ("smaug_vacio.cpp", []),
 ]
 
 
 def sources():
     # this file too: its flags are part of what the library is built from
-    return sorted(CSRC.glob("*.cu")) + sorted(CSRC.glob("*.cuh")) + sorted(CSRC.glob("*.inc")) + [
+    return sorted(CSRC.glob("*.cu")) + sorted(CSRC.glob("*.cpp")) + sorted(CSRC.glob("*.cuh")) + sorted(
+        CSRC.glob("*.inc")) + [
         PKG.parent / "include" / "smaug_b200.h", Path(__file__).resolve()]
 
 
