@@ -65,6 +65,7 @@ const char *plan_sim(const smaug_params *prm, SimPlan &r) {
     r.geo.btype[d] = d < D ? prm->btype[d] : 0;
     N *= n;
   }
+  if (N * (long long)r.NVAR >= (1LL << 31)) return "grid too large: NVAR * N must stay below 2^31";
   r.geo.st[0] = 1;
   r.geo.st[1] = r.geo.n[0];
   r.geo.st[2] = (long long)r.geo.n[0] * r.geo.n[1];

@@ -66,6 +66,13 @@ __device__ __forceinline__ float vmax(float a, float b) { return fmaxf(a, b); }
 __device__ __forceinline__ double vabs(double a) { return fabs(a); }
 __device__ __forceinline__ float vabs(float a) { return fabsf(a); }
 
+// Offset of field f at cell i in 32-bit arithmetic (the host rejects grids
+// whose NVAR * N does not fit 31 bits): one multiply-add per access instead
+// of a 64-bit product.
+__device__ __forceinline__ unsigned fo32(int f, long long N, long long i) {
+  return (unsigned)f * (unsigned)N + (unsigned)i;
+}
+
 // State accessor: evolved fields of type T, background fields FP64.
 template <int D, typename T>
 struct CellT {
@@ -74,11 +81,11 @@ struct CellT {
   long long N;
   // field f at cell i in the stencil type
   __device__ __forceinline__ T v(int f, long long i) const {
-    return f < Lay<D>::NW ? __ldg(in + (long long)f * N + i) : (T)__ldg(bg + (long long)(f - Lay<D>::NW) * N + i);
+    return f < Lay<D>::NW ? __ldg(in + fo32(f, N, i)) : (T)__ldg(bg + fo32(f - Lay<D>::NW, N, i));
   }
   // field f at cell i in FP64
   __device__ __forceinline__ double vd(int f, long long i) const {
-    return f < Lay<D>::NW ? (double)__ldg(in + (long long)f * N + i) : __ldg(bg + (long long)(f - Lay<D>::NW) * N + i);
+    return f < Lay<D>::NW ? (double)__ldg(in + fo32(f, N, i)) : __ldg(bg + fo32(f - Lay<D>::NW, N, i));
   }
 };
 
@@ -159,6 +166,44 @@ __device__ __forceinline__ void q_all(const CellT<D, T> &c, long long i, int d, 
     if (f != d) q[s++] = c.v(L::B0 + f, i);
 }
 
+// cfast/courant maxima as reduce_cell, for the mixed path: the kinetic and
+// magnetic parts are subtracted from the energy in FP64 (the pressure
+// recovery cancels), the wave speeds built from it in FP32; the maxima are
+// kept in FP64.
+template <int D>
+__device__ __forceinline__ void reduce_cell_mixed(const Geo &g, const Phys &p, const double *o, const double *b,
+                                                  long long idx, double *r) {
+  using L = Lay<D>;
+  double m2 = 0, b2 = 0, bbb = 0, bb2 = 0;
+#pragma unroll
+  for (int k = 0; k < D; ++k) {
+    m2 += o[L::M0 + k] * o[L::M0 + k];
+    b2 += o[L::B0 + k] * o[L::B0 + k];
+    bbb += b[2 + k] * o[L::B0 + k];
+    bb2 += b[2 + k] * b[2 + k];
+  }
+  const double rtd = o[L::RHO] + b[1];
+  const double pk = (p.gamma - 1) * (o[L::EN] - 0.5 * (m2 / rtd) - 0.5 * b2 - bbb);
+  // (explicitly rounded FP32 operations: never contracted, so every build
+  // variant of the stage kernel gives the same bits)
+  const float gam = (float)p.gamma, irt = (float)(1.0 / rtd);
+  const float cs2 = __fmul_rn(__fmul_rn(gam, (float)(pk + (p.gamma - 1) * (b[0] - 0.5 * bb2))), irt);
+  const float cf = __fadd_rn(__fmul_rn((float)(b2 + bb2 + 2.0 * bbb), irt), cs2);
+#pragma unroll
+  for (int d = 0; d < D; ++d) {
+    const float bd = (float)(b[2 + d] + o[L::B0 + d]);
+    const float disc = __fsub_rn(__fmul_rn(cf, cf), __fmul_rn(__fmul_rn(__fmul_rn(4.0f, cs2), __fmul_rn(bd, bd)), irt));
+    const float cfi = __fmul_rn(0.5f, __fadd_rn(cf, __fsqrt_rn(fmaxf(disc, 0.0f))));
+    const double cfd = (double)__fadd_rn(__fsqrt_rn(cfi), fabsf(__fmul_rn((float)o[L::M0 + d], irt)));
+    if (cfd > r[d] || cfd != cfd) r[d] = cfd;
+    if (d == D - 1) {
+      const double cour = cfd / __ldg(g.dxlast + idx);
+      if (cour > r[3] || cour != cour) r[3] = cour;
+      if (idx >= g.K && (cour > r[4] || cour != cour)) r[4] = cour;
+    }
+  }
+}
+
 // The end of a stage for one cell (all threads of the block call it; the
 // inactive ones only take part in the block's maxima): the stage output
 // base + h dL with the driver, the RK combination of the stage, the writes of
@@ -176,7 +221,7 @@ __device__ __forceinline__ void stage_epilogue(const StageArgs &a, const Geo &g,
     float hi[NW], lo[NW];
     if (!MIXED) {
 #pragma unroll
-      for (int f = 0; f < NW; ++f) o[f] = a.base[(long long)f * g.N + idx] + h * (double)dL[f];
+      for (int f = 0; f < NW; ++f) o[f] = a.base[fo32(f, g.N, idx)] + h * (double)dL[f];
       if (p.drv_on) {  // momentum driver on the stage output (before the RK combination)
         const double vvz = driver_vvz<D>(g, p, a.sc, a.tfrac, c);
         const double rb = __ldg(a.bg + (long long)(L::RHOB - NW) * g.N + idx);
@@ -188,12 +233,12 @@ __device__ __forceinline__ void stage_epilogue(const StageArgs &a, const Geo &g,
       if (a.kind == 3) {
 #pragma unroll
         for (int f = 0; f < NW; ++f) {
-          const long long j = (long long)f * g.N + idx;
+          const unsigned j = fo32(f, g.N, idx);
           a.acc[j] = (a.acc[j] + 2.0 * C.vd(f, idx) + o[f] - 4.0 * a.base[j]) * (1.0 / 3.0);
         }
       } else if (a.kind == 4) {
 #pragma unroll
-        for (int f = 0; f < NW; ++f) o[f] += a.acc[(long long)f * g.N + idx];
+        for (int f = 0; f < NW; ++f) o[f] += a.acc[fo32(f, g.N, idx)];
       }
     } else {
       // RK4 in increment form, W = w32 + c32:
@@ -214,7 +259,7 @@ __device__ __forceinline__ void stage_epilogue(const StageArgs &a, const Geo &g,
       }
 #pragma unroll
       for (int f = 0; f < NW; ++f) {
-        const long long j = (long long)f * g.N + idx;
+        const unsigned j = fo32(f, g.N, idx);
         const double inc = incs[f];
         if (a.kind == 4) {
           const double wn = ((double)a.w32[j] + (double)a.c32[j]) + (inc + (double)a.acc32[j]);
@@ -252,21 +297,24 @@ __device__ __forceinline__ void stage_epilogue(const StageArgs &a, const Geo &g,
       const long long j = gidx<D>(g, cc);
       if (!MIXED) {
 #pragma unroll
-        for (int f = 0; f < NW; ++f) a.out[(long long)f * g.N + j] = o[f];
+        for (int f = 0; f < NW; ++f) a.out[fo32(f, g.N, j)] = o[f];
       } else if (a.kind == 4) {
 #pragma unroll
         for (int f = 0; f < NW; ++f) {
-          a.w32[(long long)f * g.N + j] = hi[f];
-          a.c32[(long long)f * g.N + j] = lo[f];
+          a.w32[fo32(f, g.N, j)] = hi[f];
+          a.c32[fo32(f, g.N, j)] = lo[f];
         }
       } else {
 #pragma unroll
-        for (int f = 0; f < NW; ++f) a.out32[(long long)f * g.N + j] = hi[f];
+        for (int f = 0; f < NW; ++f) a.out32[fo32(f, g.N, j)] = hi[f];
       }
       double bgv[NB];
 #pragma unroll
-      for (int b = 0; b < NB; ++b) bgv[b] = __ldg(a.bg + (long long)b * g.N + j);
-      reduce_cell<D>(g, p, o, bgv, j, red);
+      for (int b = 0; b < NB; ++b) bgv[b] = __ldg(a.bg + fo32(b, g.N, j));
+      if (MIXED)
+        reduce_cell_mixed<D>(g, p, o, bgv, j, red);
+      else
+        reduce_cell<D>(g, p, o, bgv, j, red);
     }
   }
   block_max_flush<6>(red, &a.sc->red[a.red_out]);

@@ -226,16 +226,22 @@ __device__ __forceinline__ void tile_body2(const StageArgs &a, const Geo &g, con
       const int sq = fo == 0 ? 1 : B::QX;                    // q stride along fo
       const long long sgf = g.st[fo];
       const T dxd = (T)__ldg(g.dx1[d] + c[d]);
+      // dx c_max c_hyp of each slot, and whether the neighbours along fo are
+      // inner cells (the cell itself is: tiles cover inner cells only)
+      T kk[5];
+#pragma unroll
+      for (int k = 0; k < 5; ++k) {
+        const int fid = k == 0 ? L::RHO : k == 1 ? L::EN : k < 4 ? L::M0 + (k - 2) : L::B0 + (d == 0 ? 1 : 0);
+        kk[k] = dxd * cm[d] * (T)p.chyp[fid];
+      }
+      const int cfo = c[fo], nfo = fo == 0 ? n0 : n1;
+      const bool inm = cfo - 1 >= 2, inp = cfo + 1 <= nfo - 3;
       // nu_R, nu_L of slot k at the cell shifted by s (-1, 0, +1) along fo;
       // 0 off the inner cells, as the reference's viscosity arrays are
       auto nu_at = [&](int k, int s, T &nr, T &nl) {
-        int cc[3] = {c[0], c[1], 0};
-        cc[fo] += s;
-        const bool in = cc[0] >= 2 && cc[0] <= n0 - 3 && cc[1] >= 2 && cc[1] <= n1 - 3;
-        const int fid = k == 0 ? L::RHO : k == 1 ? L::EN : k < 4 ? L::M0 + (k - 2) : L::B0 + (d == 0 ? 1 : 0);
-        const T kk = dxd * cm[d] * (T)p.chyp[fid];
-        nr = in ? kk * V[k * vn + fr + s * sv] : T(0);
-        nl = in ? kk * V[k * vn + fl + s * sv] : T(0);
+        const bool in = s == 0 ? true : (s > 0 ? inp : inm);
+        nr = in ? kk[k] * V[k * vn + fr + s * sv] : T(0);
+        nl = in ? kk[k] * V[k * vn + fl + s * sv] : T(0);
       };
 #pragma unroll
       for (int k = 0; k < 5; ++k) {
