@@ -193,9 +193,10 @@ __device__ __forceinline__ void tile_body2(const StageArgs &a, const Geo &g, con
       }
     }
     const int r0 = (tx + 3) + B::QX * (ty + 3);
-#pragma unroll
-    for (int d = 0; d < 2; ++d) {
-      if (!p.hyperdif && !p.has_bgb) break;
+    // the terms along dimension d (a compile-time constant in each call, so
+    // that nothing indexes Geo, c, cm or idx1 dynamically)
+    auto dim_terms = [&](auto dc) {
+      constexpr int d = decltype(dc)::value;
       const int sd = d == 0 ? 1 : B::QX;
       const long long sg = g.st[d];
       const bool zd = z1(g, c, d);
@@ -214,7 +215,7 @@ __device__ __forceinline__ void tile_body2(const StageArgs &a, const Geo &g, con
           dL[L::EN] += C.v(L::BB0 + d, idx) * C.v(L::BB0 + dir, idx) * gv;
         }
       }
-      if (!p.hyperdif) continue;
+      if (!p.hyperdif) return;
       // this dimension's face ratios: the cell's right face, its left face,
       // and the face stride across d (the other dim)
       const T *V = d == 0 ? V0 : V1;
@@ -326,6 +327,10 @@ __device__ __forceinline__ void tile_body2(const StageArgs &a, const Geo &g, con
         dL[L::B0 + f] += (nr * dbp - nl * dbm) * i2;
         dL[L::EN] += ((T)0.5 * (b[0] + b[sd]) * nr * dbp - (T)0.5 * (b[0] + b[-sd]) * nl * dbm) * i2;
       }
+    };
+    if (p.hyperdif || p.has_bgb) {
+      dim_terms(std::integral_constant<int, 0>{});
+      dim_terms(std::integral_constant<int, 1>{});
     }
   }
   stage_epilogue<2, T>(a, g, p, C, c, active, idx, h, dL, numax);
