@@ -61,6 +61,15 @@ __device__ __forceinline__ void block_max_flush(double *v, Reduce *r) {
   }
 }
 
+// The same for FP32 running maxima (widened exactly to FP64).
+template <int NV>
+__device__ __forceinline__ void block_max_flush(const float *v, Reduce *r) {
+  double w[NV];
+#pragma unroll
+  for (int k = 0; k < NV; ++k) w[k] = (double)v[k];
+  block_max_flush<NV>(w, r);
+}
+
 // Coordinates along d that receive the value of inner coordinate x: x itself
 // plus its ghost image (periodic wrap, boundary{0,1,2}_per_parallel; or the
 // contcd4 copies 0<-4, 1<-3, n-1<-n-5, n-2<-n-4, boundary{0,1,2}_contcd4_parallel

@@ -99,9 +99,10 @@ __device__ __forceinline__ bool in_grid(const Geo &g, const int *c) {
 
 // Fluxes along dir with reciprocal arithmetic (the same physical fluxes as
 // fluxes_at): rho, momentum, energy, induction.  rho_t, its reciprocal and
-// the total pressure are formed in FP64.
+// the total pressure are formed in FP64.  bgb = 0: e_b and B_b are zero
+// everywhere (not read).
 template <int D, typename T>
-__device__ __forceinline__ void fluxes_fast(const CellT<D, T> &c, long long i, int dir, double gam, T *F) {
+__device__ __forceinline__ void fluxes_fast(const CellT<D, T> &c, long long i, int dir, double gam, bool bgb, T *F) {
   using L = Lay<D>;
   const T rho = c.v(L::RHO, i);
   const double rt = (double)rho + c.vd(L::RHOB, i);
@@ -112,9 +113,9 @@ __device__ __forceinline__ void fluxes_fast(const CellT<D, T> &c, long long i, i
   for (int k = 0; k < D; ++k) {
     m[k] = c.v(L::M0 + k, i);
     b[k] = c.v(L::B0 + k, i);
-    bb[k] = c.v(L::BB0 + k, i);
+    bb[k] = bgb ? c.v(L::BB0 + k, i) : T(0);
   }
-  const T e = c.v(L::EN, i), eb = c.v(L::EB, i);
+  const T e = c.v(L::EN, i), eb = bgb ? c.v(L::EB, i) : T(0);
   double bbb = 0, b2 = 0, m2 = 0;
   T bbm = 0, bm = 0;
 #pragma unroll
@@ -166,56 +167,65 @@ __device__ __forceinline__ void q_all(const CellT<D, T> &c, long long i, int d, 
     if (f != d) q[s++] = c.v(L::B0 + f, i);
 }
 
-// cfast/courant maxima as reduce_cell, for the mixed path: the kinetic and
-// magnetic parts are subtracted from the energy in FP64 (the pressure
-// recovery cancels), the wave speeds built from it in FP32; the maxima are
-// kept in FP64.
+// cfast/courant maxima as reduce_cell (computec3, dervfields.cu:241-309), for
+// the mixed path: the state is FP32 there, so the wave speeds are formed in
+// FP32 from a correctly rounded reciprocal of rho_t (the pressure recovery's
+// rounding stays at the level of the FP32 inputs); the courant number divides
+// by the metric through a correctly rounded reciprocal too.  Explicitly
+// rounded operations, never contracted: every build variant of the stage
+// kernel gives the same bits.  b: eb, rho_b, B_b (zeros when the simulation
+// has no energy background).  The maxima are FP32 values and kept in FP32.
 template <int D>
 __device__ __forceinline__ void reduce_cell_mixed(const Geo &g, const Phys &p, const double *o, const double *b,
-                                                  long long idx, double *r) {
+                                                  long long idx, float *r) {
   using L = Lay<D>;
-  double m2 = 0, b2 = 0, bbb = 0, bb2 = 0;
+  const float irt = __frcp_rn((float)(o[L::RHO] + b[1]));
+  float m2 = 0.0f, b2 = 0.0f, bbb = 0.0f, bb2 = 0.0f;
 #pragma unroll
   for (int k = 0; k < D; ++k) {
-    m2 += o[L::M0 + k] * o[L::M0 + k];
-    b2 += o[L::B0 + k] * o[L::B0 + k];
-    bbb += b[2 + k] * o[L::B0 + k];
-    bb2 += b[2 + k] * b[2 + k];
+    const float m = (float)o[L::M0 + k], bf = (float)o[L::B0 + k], bb = (float)b[2 + k];
+    m2 = __fmaf_rn(m, m, m2);
+    b2 = __fmaf_rn(bf, bf, b2);
+    bbb = __fmaf_rn(bb, bf, bbb);
+    bb2 = __fmaf_rn(bb, bb, bb2);
   }
-  const double rtd = o[L::RHO] + b[1];
-  const double pk = (p.gamma - 1) * (o[L::EN] - 0.5 * (m2 / rtd) - 0.5 * b2 - bbb);
-  // (explicitly rounded FP32 operations: never contracted, so every build
-  // variant of the stage kernel gives the same bits)
-  const float gam = (float)p.gamma, irt = (float)(1.0 / rtd);
-  const float cs2 = __fmul_rn(__fmul_rn(gam, (float)(pk + (p.gamma - 1) * (b[0] - 0.5 * bb2))), irt);
-  const float cf = __fadd_rn(__fmul_rn((float)(b2 + bb2 + 2.0 * bbb), irt), cs2);
+  const float gm1 = (float)(p.gamma - 1.0), gam = (float)p.gamma;
+  // p_k = (gamma-1) (e - m^2/(2 rho_t) - B^2/2 - B.B_b)
+  const float ek = __fsub_rn(__fsub_rn(__fsub_rn((float)o[L::EN], __fmul_rn(__fmul_rn(0.5f, m2), irt)),
+                                       __fmul_rn(0.5f, b2)), bbb);
+  const float pk = __fmul_rn(gm1, ek);
+  // c_s^2 = gamma (p_k + (gamma-1)(e_b - B_b^2/2)) / rho_t
+  const float pbg = __fmul_rn(gm1, __fsub_rn((float)b[0], __fmul_rn(0.5f, bb2)));
+  const float cs2 = __fmul_rn(__fmul_rn(gam, __fadd_rn(pk, pbg)), irt);
+  const float cf = __fadd_rn(__fmul_rn(__fadd_rn(__fadd_rn(b2, bb2), __fmul_rn(2.0f, bbb)), irt), cs2);
 #pragma unroll
   for (int d = 0; d < D; ++d) {
     const float bd = (float)(b[2 + d] + o[L::B0 + d]);
     const float disc = __fsub_rn(__fmul_rn(cf, cf), __fmul_rn(__fmul_rn(__fmul_rn(4.0f, cs2), __fmul_rn(bd, bd)), irt));
     const float cfi = __fmul_rn(0.5f, __fadd_rn(cf, __fsqrt_rn(fmaxf(disc, 0.0f))));
-    const double cfd = (double)__fadd_rn(__fsqrt_rn(cfi), fabsf(__fmul_rn((float)o[L::M0 + d], irt)));
-    if (cfd > r[d] || cfd != cfd) r[d] = cfd;
+    const float cff = __fadd_rn(__fsqrt_rn(cfi), fabsf(__fmul_rn((float)o[L::M0 + d], irt)));
+    if (cff > r[d] || cff != cff) r[d] = cff;
     if (d == D - 1) {
-      const double cour = cfd / __ldg(g.dxlast + idx);
+      const float cour = __fmul_rn(cff, __frcp_rn((float)__ldg(g.dxlast + idx)));
       if (cour > r[3] || cour != cour) r[3] = cour;
       if (idx >= g.K && (cour > r[4] || cour != cour)) r[4] = cour;
     }
   }
 }
 
-// The end of a stage for one cell (all threads of the block call it; the
-// inactive ones only take part in the block's maxima): the stage output
-// base + h dL with the driver, the RK combination of the stage, the writes of
-// the cell and its ghost images, and the wave-speed / viscosity maxima.
+// The end of a stage for one cell: the stage output base + h dL with the
+// driver, the RK combination of the stage, the writes of the cell and its
+// ghost images, and the wave-speed / viscosity maxima, taken into the
+// thread's running maxima red[6] (in the stencil type: FP32 values in the
+// mixed path; the caller flushes them to the simulation's reduction slot).
 template <int D, typename T>
 __device__ __forceinline__ void stage_epilogue(const StageArgs &a, const Geo &g, const Phys &p, const CellT<D, T> &C,
                                                const int *c, bool active, long long idx, double h, const T *dL,
-                                               T numax) {
+                                               T numax, T *red) {
   using L = Lay<D>;
   constexpr int NW = L::NW, NB = L::NVAR - NW;
   constexpr bool MIXED = sizeof(T) == sizeof(float);
-  double red[6] = {0, 0, 0, 0, 0, (double)numax};
+  if (numax > red[5] || numax != numax) red[5] = numax;
   if (active) {
     double o[NW];
     float hi[NW], lo[NW];
@@ -308,16 +318,18 @@ __device__ __forceinline__ void stage_epilogue(const StageArgs &a, const Geo &g,
 #pragma unroll
         for (int f = 0; f < NW; ++f) a.out32[fo32(f, g.N, j)] = hi[f];
       }
+      // backgrounds (e_b and B_b are zero everywhere without an energy
+      // background: only rho_b is read then)
       double bgv[NB];
 #pragma unroll
-      for (int b = 0; b < NB; ++b) bgv[b] = __ldg(a.bg + fo32(b, g.N, j));
-      if (MIXED)
+      for (int b = 0; b < NB; ++b)
+        bgv[b] = (b == L::RHOB - NW || p.has_bgb) ? __ldg(a.bg + fo32(b, g.N, j)) : 0.0;
+      if constexpr (MIXED)
         reduce_cell_mixed<D>(g, p, o, bgv, j, red);
       else
         reduce_cell<D>(g, p, o, bgv, j, red);
     }
   }
-  block_max_flush<6>(red, &a.sc->red[a.red_out]);
 }
 
 // One RK stage on the tile (bx, by, bz) of one simulation; every thread of
@@ -325,7 +337,7 @@ __device__ __forceinline__ void stage_epilogue(const StageArgs &a, const Geo &g,
 // elements of T.
 template <int D, typename T, typename S>
 __device__ __forceinline__ void tile_body(const StageArgs &a, const Geo &g, const Phys &p, int bx, int by, int bz,
-                                          T *sm) {
+                                          T *sm, T *red) {
   using L = Lay<D>;
   constexpr int TX = S::TX, TY = S::TY, TZ = S::TZ, NT = TX * TY * TZ;
   constexpr int NW = L::NW, NB = L::NVAR - NW;
@@ -373,7 +385,7 @@ __device__ __forceinline__ void tile_body(const StageArgs &a, const Geo &g, cons
       box.at(r, cc);
       T F[NW];
       if (in_grid<D>(g, cc)) {
-        fluxes_fast<D, T>(C, gidx<D>(g, cc), dir, p.gamma, F);
+        fluxes_fast<D, T>(C, gidx<D>(g, cc), dir, p.gamma, p.has_bgb, F);
       } else {
 #pragma unroll
         for (int f = 0; f < NW; ++f) F[f] = 0;
@@ -620,14 +632,16 @@ __device__ __forceinline__ void tile_body(const StageArgs &a, const Geo &g, cons
     __syncthreads();
   }
 
-  stage_epilogue<D, T>(a, g, p, C, c, active, idx, h, dL, numax);
+  stage_epilogue<D, T>(a, g, p, C, c, active, idx, h, dL, numax, red);
 }
 
 // One launch = one RK stage of one simulation, one block per tile.
 template <int D, typename T>
 __global__ void __launch_bounds__(256, 2) tile_stage_kernel(StageArgs a, Geo g, Phys p) {
   extern __shared__ __align__(16) unsigned char smraw[];
-  tile_body<D, T, TileShape<D>>(a, g, p, blockIdx.x, blockIdx.y, blockIdx.z, reinterpret_cast<T *>(smraw));
+  T red[6] = {0, 0, 0, 0, 0, 0};
+  tile_body<D, T, TileShape<D>>(a, g, p, blockIdx.x, blockIdx.y, blockIdx.z, reinterpret_cast<T *>(smraw), red);
+  block_max_flush<6>(red, &a.sc->red[a.red_out]);
 }
 
 // shared memory elements (of the stencil type) the tile body needs

@@ -62,7 +62,8 @@ struct Box2 {
 };
 
 template <typename T, typename S>
-__device__ __forceinline__ void tile_body2(const StageArgs &a, const Geo &g, const Phys &p, int bx, int by, T *sm) {
+__device__ __forceinline__ void tile_body2(const StageArgs &a, const Geo &g, const Phys &p, int bx, int by, T *sm,
+                                           T *red) {
   constexpr int D = 2;
   using L = Lay<2>;
   using B = Box2<S>;
@@ -90,7 +91,7 @@ __device__ __forceinline__ void tile_body2(const StageArgs &a, const Geo &g, con
     const int cy = dir == 0 ? oy + rr / B::F0X : oy - 2 + rr / B::F1X;
     T F[NW];
     if (cx >= 0 && cx < n0 && cy >= 0 && cy < n1) {
-      fluxes_fast<2, T>(C, cx + (long long)cy * g.st[1], dir, p.gamma, F);
+      fluxes_fast<2, T>(C, cx + (long long)cy * g.st[1], dir, p.gamma, p.has_bgb, F);
     } else {
 #pragma unroll
       for (int f = 0; f < NW; ++f) F[f] = 0;
@@ -333,7 +334,7 @@ __device__ __forceinline__ void tile_body2(const StageArgs &a, const Geo &g, con
       dim_terms(std::integral_constant<int, 1>{});
     }
   }
-  stage_epilogue<2, T>(a, g, p, C, c, active, idx, h, dL, numax);
+  stage_epilogue<2, T>(a, g, p, C, c, active, idx, h, dL, numax, red);
 }
 
 // Shared memory (elements of the stencil type) of a stage body: the
