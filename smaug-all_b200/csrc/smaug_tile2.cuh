@@ -26,13 +26,15 @@
 namespace SMAUG_NS {
 using namespace smaug;
 
-// The six q values of one cell (2-D): slot 0 rho, 1 internal energy (FP64),
-// 2 v_x, 3 v_y, 4 B_x, 5 B_y.
+// The q slots of one cell (2-D): the hyperviscosity inputs, slot 0 rho,
+// 1 internal energy (FP64), 2 v_x, 3 v_y, 4 B_x, 5 B_y; then what the
+// momentum terms read at the neighbours: 6 rho_t = rho + rho_b, 7 m_x, 8 m_y.
 template <typename T>
-__device__ __forceinline__ void q_six(const CellT<2, T> &c, long long i, T *q) {
+__device__ __forceinline__ void q_cell(const CellT<2, T> &c, long long i, T *q) {
   using L = Lay<2>;
   const T rho = c.v(L::RHO, i);
-  const double irtd = 1.0 / ((double)rho + c.vd(L::RHOB, i));
+  const double rhob = c.vd(L::RHOB, i);
+  const double irtd = 1.0 / ((double)rho + rhob);
   const T irt = (T)irtd;
   const T m0 = c.v(L::M0, i), m1 = c.v(L::M0 + 1, i), b0 = c.v(L::B0, i), b1 = c.v(L::B0 + 1, i);
   const double b2 = (double)b0 * (double)b0 + (double)b1 * (double)b1;
@@ -43,12 +45,18 @@ __device__ __forceinline__ void q_six(const CellT<2, T> &c, long long i, T *q) {
   q[3] = m1 * irt;
   q[4] = b0;
   q[5] = b1;
+  q[6] = rho + (T)rhob;
+  q[7] = m0;
+  q[8] = m1;
 }
 
 // Box sizes of the three-phase body for a TX x TY tile.
 template <typename S>
 struct Box2 {
   static constexpr int TX = S::TX, TY = S::TY;
+  // flux slots: the evolved fields but B_d (its flux along d is zero)
+  static constexpr int NF = Lay<2>::NW - 1;
+  static constexpr int NQS = 9;  // q slots per cell (q_cell)
   static constexpr int F0X = TX + 4, F0N = F0X * TY;           // x-fluxes: tile +-2 along x
   static constexpr int F1X = TX, F1N = TX * (TY + 4);          // y-fluxes: tile +-2 along y
   static constexpr int QX = TX + 6, QN = QX * (TY + 6);        // q: tile +-3
@@ -57,7 +65,9 @@ struct Box2 {
   // face ratios along y: faces y+1/2 for y in [-1, TY), columns tile +-1
   static constexpr int V1X = TX + 2, V1N = (TX + 2) * (TY + 1);
   // offsets (elements) of the arrays in shared memory
-  static constexpr int OF0 = 0, OF1 = OF0 + 6 * F0N, OQ = OF1 + 6 * F1N, OV0 = OQ + 6 * QN, OV1 = OV0 + 5 * V0N;
+  static constexpr int OF0 = 0, OF1 = OF0 + NF * F0N, OQ = OF1 + NF * F1N, OV0 = OQ + NQS * QN, OV1 = OV0 + 5 * V0N;
+  // flux slot of field f along dir
+  static constexpr __host__ __device__ int fslot(int f, int dir) { return f < Lay<2>::B0 + dir ? f : f - 1; }
   static constexpr int ELEMS = OV1 + 5 * V1N;
 };
 
@@ -99,7 +109,8 @@ __device__ __forceinline__ void tile_body2(const StageArgs &a, const Geo &g, con
     T *dst = (dir == 0 ? F0 : F1) + rr;
     constexpr int stride = dir == 0 ? B::F0N : B::F1N;
 #pragma unroll
-    for (int f = 0; f < NW; ++f) dst[f * stride] = F[f];
+    for (int f = 0; f < NW; ++f)
+      if (f != L::B0 + dir) dst[B::fslot(f, dir) * stride] = F[f];
   };
   for (int r = t; r < B::F0N + B::F1N + B::QN; r += NT) {
     if (r < B::F0N) {
@@ -109,19 +120,20 @@ __device__ __forceinline__ void tile_body2(const StageArgs &a, const Geo &g, con
     } else {
       const int rr = r - B::F0N - B::F1N;
       int cx = ox - 3 + rr % B::QX, cy = oy - 3 + rr / B::QX;
-      T q[6];
+      T q[B::NQS];
       const bool inx = cx >= 0 && cx < n0, iny = cy >= 0 && cy < n1;
       // pads of the padded copies: right 0, left q(5); corners never read
+      // (slots 6..8 are read at the tile +-1 only, always inside the grid)
       if ((!inx && !iny) || cx >= n0 || cy >= n1) {
 #pragma unroll
-        for (int k = 0; k < 6; ++k) q[k] = 0;
+        for (int k = 0; k < B::NQS; ++k) q[k] = 0;
       } else {
         if (cx < 0) cx = 5;
         if (cy < 0) cy = 5;
-        q_six<T>(C, cx + (long long)cy * g.st[1], q);
+        q_cell<T>(C, cx + (long long)cy * g.st[1], q);
       }
 #pragma unroll
-      for (int k = 0; k < 6; ++k) Q[k * B::QN + rr] = q[k];
+      for (int k = 0; k < B::NQS; ++k) Q[k * B::QN + rr] = q[k];
     }
   }
   __syncthreads();
@@ -180,7 +192,8 @@ __device__ __forceinline__ void tile_body2(const StageArgs &a, const Geo &g, con
       const T w12 = idx1[dir] * (T)(1.0 / 12.0);
 #pragma unroll
       for (int f = 0; f < NW; ++f) {
-        const T *Fp = Fb + f * fs;
+        if (f == L::B0 + dir) continue;  // zero flux
+        const T *Fp = Fb + B::fslot(f, dir) * fs;
         dL[f] -= ((T)8 * (Fp[st] - Fp[-st]) - (Fp[2 * st] - Fp[-2 * st])) * w12;
       }
     }
@@ -199,7 +212,6 @@ __device__ __forceinline__ void tile_body2(const StageArgs &a, const Geo &g, con
     auto dim_terms = [&](auto dc) {
       constexpr int d = decltype(dc)::value;
       const int sd = d == 0 ? 1 : B::QX;
-      const long long sg = g.st[d];
       const bool zd = z1(g, c, d);
       const T i1 = idx1[d], i2 = idx1[d] * idx1[d];
       if (p.has_bgb) {  // background energy terms along d (addenergyterms_cd2)
@@ -226,7 +238,6 @@ __device__ __forceinline__ void tile_body2(const StageArgs &a, const Geo &g, con
       const int fo = 1 - d;                                  // the other dimension
       const int sv = d == 0 ? B::V0X : 1;                    // face stride along fo
       const int sq = fo == 0 ? 1 : B::QX;                    // q stride along fo
-      const long long sgf = g.st[fo];
       const T dxd = (T)__ldg(g.dx1[d] + c[d]);
       // dx c_max c_hyp of each slot, and whether the neighbours along fo are
       // inner cells (the cell itself is: tiles cover inner cells only)
@@ -260,10 +271,9 @@ __device__ __forceinline__ void tile_body2(const StageArgs &a, const Geo &g, con
         const T dp = zd ? T(0) : q[sd] - q[0], dm = zd ? T(0) : q[0] - q[-sd];
         dL[k == 0 ? L::RHO : L::EN] += (nr * dp - nl * dm) * i2;
       }
-      // momentum
-      const T rt0 = C.v(L::RHO, idx) + C.v(L::RHOB, idx);
-      const T rtp = C.v(L::RHO, idx + sg) + C.v(L::RHOB, idx + sg);
-      const T rtm = C.v(L::RHO, idx - sg) + C.v(L::RHOB, idx - sg);
+      // momentum (rho_t and m at the neighbours from the q box)
+      const T *qrt = Q + 6 * B::QN + r0;
+      const T rt0 = qrt[0], rtp = qrt[sd], rtm = qrt[-sd];
 #pragma unroll
       for (int f = 0; f < 2; ++f) {
         const int k = 2 + f;
@@ -271,7 +281,8 @@ __device__ __forceinline__ void tile_body2(const StageArgs &a, const Geo &g, con
         T nr, nl;
         nu_at(k, 0, nr, nl);
         const T dvp = zd ? T(0) : v[sd] - v[0], dvm = zd ? T(0) : v[0] - v[-sd];
-        const T m0 = C.v(L::M0 + f, idx), mp = C.v(L::M0 + f, idx + sg), mm = C.v(L::M0 + f, idx - sg);
+        const T *qm = Q + (7 + f) * B::QN + r0;
+        const T m0 = qm[0], mp = qm[sd], mm = qm[-sd];
         const T fac = (f == d ? (T)1 : (T)0.5) * i2;
         dL[L::M0 + f] += ((rt0 + rtp) * nr * dvp - (rt0 + rtm) * nl * dvm) * (T)0.5 * fac;
         dL[L::EN] += ((m0 + mp) * nr * dvp - (m0 + mm) * nl * dvm) * (T)0.5 * fac;
@@ -280,7 +291,6 @@ __device__ __forceinline__ void tile_body2(const StageArgs &a, const Geo &g, con
 #pragma unroll
           for (int s = 0; s < 2; ++s) {
             const int o = s ? sq : -sq;
-            const long long go = s ? sgf : -sgf;
             int cx[3] = {c[0], c[1], 0};
             cx[f] += s ? 1 : -1;
             T nr2, nl2;
@@ -288,8 +298,8 @@ __device__ __forceinline__ void tile_body2(const StageArgs &a, const Geo &g, con
             const T nsum = nr2 + nl2;
             const T tmp5 = z1(g, cx, d) ? T(0) : (v[o + sd] - v[o - sd]) * (T)0.5 * i1;
             const T tmp6 = tmp5 * nsum * (T)0.25;
-            t1[s] = (C.v(L::RHO, idx + go) + C.v(L::RHOB, idx + go)) * tmp6;
-            t2[s] = tmp6 * C.v(L::M0 + d, idx + go);
+            t1[s] = qrt[o] * tmp6;
+            t2[s] = tmp6 * Q[(7 + d) * B::QN + r0 + o];
           }
           if (!z1(g, c, f)) {
             const T hf = (T)0.5 * idx1[f];
@@ -308,7 +318,6 @@ __device__ __forceinline__ void tile_body2(const StageArgs &a, const Geo &g, con
 #pragma unroll
         for (int s = 0; s < 2; ++s) {  // off-diagonal: B_d -= d_f( (nu_L+nu_R)/2 d_d B_f ), e with B_d
           const int o = s ? sq : -sq;
-          const long long go = s ? sgf : -sgf;
           int cx[3] = {c[0], c[1], 0};
           cx[f] += s ? 1 : -1;
           T nr2, nl2;
@@ -316,7 +325,7 @@ __device__ __forceinline__ void tile_body2(const StageArgs &a, const Geo &g, con
           const T nsum = nr2 + nl2;
           const T tmp2 = z1(g, cx, d) ? T(0) : (b[o + sd] - b[o - sd]) * (T)0.5 * i1;
           t1[s] = tmp2 * nsum * (T)0.5;
-          t2[s] = t1[s] * C.v(L::B0 + d, idx + go);
+          t2[s] = t1[s] * Q[(4 + d) * B::QN + r0 + o];
         }
         if (!z1(g, c, f)) {
           const T hf = (T)0.5 * idx1[f];
