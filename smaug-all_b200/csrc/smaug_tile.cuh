@@ -65,6 +65,13 @@ __device__ __forceinline__ double vmax(double a, double b) { return fmax(a, b); 
 __device__ __forceinline__ float vmax(float a, float b) { return fmaxf(a, b); }
 __device__ __forceinline__ double vabs(double a) { return fabs(a); }
 __device__ __forceinline__ float vabs(float a) { return fabsf(a); }
+// a * b + c with one rounding (never left to contraction)
+__device__ __forceinline__ double vfma(double a, double b, double c) { return __fma_rn(a, b, c); }
+__device__ __forceinline__ float vfma(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+// The hyperviscosity ratio a / b (b > 0): IEEE division in FP64; in FP32 the
+// reciprocal-based quotient (within 2 ulp), the ratio being a limiter weight.
+__device__ __forceinline__ double vratio(double a, double b) { return a / b; }
+__device__ __forceinline__ float vratio(float a, float b) { return __fdividef(a, b); }
 
 // Offset of field f at cell i in 32-bit arithmetic (the host rejects grids
 // whose NVAR * N does not fit 31 bits): one multiply-add per access instead

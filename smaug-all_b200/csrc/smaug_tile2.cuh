@@ -7,11 +7,12 @@
 //            tile +-2 along x, y-fluxes on the tile +-2 along y, and the six
 //            hyperviscosity inputs q (rho, e_int, v_x, v_y, B_x, B_y) on the
 //            tile +-3 in both dimensions;
-//   phase B  one loop over the cell faces of both dimensions: the ratio
+//   phase B  one loop over runs of cell faces of both dimensions: the ratio
 //            max|d3 q| / max|d1 q| of the hyperviscosity once per face
 //            (nu_R of a cell and nu_L of its right neighbour share their
-//            windows), along x on the tile +-1 in y, along y on the tile +-1
-//            in x (the off-diagonal terms need nu there);
+//            windows, consecutive faces share their differences), along x on
+//            the tile +-1 in y, along y on the tile +-1 in x (the
+//            off-diagonal terms need nu there);
 //   phase C  per cell: nu = dx c_max c_hyp * ratio on the cell's faces,
 //            divergences, gravity, background energy terms, hyperdiffusion,
 //            then the shared epilogue.
@@ -139,37 +140,61 @@ __device__ __forceinline__ void tile_body2(const StageArgs &a, const Geo &g, con
   __syncthreads();
 
   // ------------------------------------------------ phase B: face ratios along x and y
-  auto face_item = [=](auto dc, int rr) {
+  // One work unit: SEG consecutive faces along d of one q slot on one line of
+  // the tile.  The line's q values are read once, each first difference
+  // |q_j+1 - q_j| and third difference |3 (q_j+1 - q_j) - (q_j+2 - q_j-1)| is
+  // formed once, and each face takes the max of the five first and the three
+  // third differences around it.  The last run of a line is shifted back to
+  // end at the line's last face (faces it shares with the run before are
+  // written twice, with the same value).
+  constexpr int SEG = 5;
+  constexpr int NS0 = (TX + 1 + SEG - 1) / SEG, NS1 = (TY + 1 + SEG - 1) / SEG;
+  constexpr int NU0 = 5 * (TY + 2) * NS0, NU1 = 5 * (TX + 2) * NS1;
+  static_assert(SEG <= TX + 1 && SEG <= TY + 1, "a run must fit in a line");
+  auto face_run = [=](auto dc, int u) {
     constexpr int d = decltype(dc)::value;
-    // the face between cells (cx, cy) and its right neighbour along d
-    const int cx = d == 0 ? ox - 1 + rr % B::V0X : ox - 1 + rr % B::V1X;
-    const int cy = d == 0 ? oy - 1 + rr / B::V0X : oy - 1 + rr / B::V1X;
-    const int rq = (cx - ox + 3) + B::QX * (cy - oy + 3);
+    constexpr int NL = d == 0 ? TX : TY;  // faces of a line: -1 .. NL-1 (tile-relative left cell)
+    int line, s, k;  // line: the row (d = 0) or column (d = 1) + 1, tile-relative
+    if (d == 0) {
+      s = u % NS0;
+      line = (u / NS0) % (TY + 2);
+      k = u / (NS0 * (TY + 2));
+    } else {
+      line = u % (TX + 2);
+      s = (u / (TX + 2)) % NS1;
+      k = u / ((TX + 2) * NS1);
+    }
+    const int f0 = min(-1 + s * SEG, NL - SEG);      // first face of the run
+    const int slot = k < 4 ? k : (d == 0 ? 5 : 4);   // B_f, f != d
     constexpr int sd = d == 0 ? 1 : B::QX;
-    T *dst = (d == 0 ? V0 : V1) + rr;
-    constexpr int stride = d == 0 ? B::V0N : B::V1N;
+    // q at the cells f0-2 .. f0+SEG+2 along d
+    const T *qq = Q + slot * B::QN +
+                  (d == 0 ? (f0 + 1) + B::QX * (line + 2) : (line + 2) + B::QX * (f0 + 1));
+    T q[SEG + 5], t1[SEG + 4], t3[SEG + 3];
 #pragma unroll
-    for (int k = 0; k < 5; ++k) {
-      const int slot = k < 4 ? k : (d == 0 ? 5 : 4);  // B_f, f != d
-      const T *qq = Q + slot * B::QN + rq;
-      T qv[6];  // q at the face's cells -2 .. +3
+    for (int j = 0; j < SEG + 5; ++j) q[j] = qq[j * sd];
 #pragma unroll
-      for (int o = -2; o <= 3; ++o) qv[o + 2] = qq[o * sd];
-      T m3 = 0, m1 = 0;
+    for (int j = 0; j < SEG + 4; ++j) t1[j] = q[j + 1] - q[j];
 #pragma unroll
-      for (int s2 = -1; s2 <= 1; ++s2)
-        m3 = vmax(m3, vabs((T)3 * (qv[s2 + 3] - qv[s2 + 2]) - (qv[s2 + 4] - qv[s2 + 1])));
+    for (int j = 1; j <= SEG + 2; ++j) t3[j] = vabs(vfma((T)3, t1[j], -(q[j + 2] - q[j - 1])));
+    T *dst = (d == 0 ? V0 + k * B::V0N : V1 + k * B::V1N);
 #pragma unroll
-      for (int s2 = -2; s2 <= 2; ++s2) m1 = vmax(m1, vabs(qv[s2 + 3] - qv[s2 + 2]));
-      dst[k * stride] = m1 > 0 ? m3 / m1 : T(0);
+    for (int m = 0; m < SEG; ++m) {
+      T m1 = 0, m3 = 0;
+#pragma unroll
+      for (int j = m; j <= m + 4; ++j) m1 = vmax(m1, vabs(t1[j]));
+#pragma unroll
+      for (int j = m + 1; j <= m + 3; ++j) m3 = vmax(m3, t3[j]);
+      const int fc = f0 + m + 1;
+      dst[d == 0 ? fc + B::V0X * line : line + B::V1X * fc] = m1 > 0 ? vratio(m3, m1) : T(0);
     }
   };
   if (p.hyperdif) {
-    for (int r = t; r < B::V0N + B::V1N; r += NT) {
-      if (r < B::V0N)
-        face_item(std::integral_constant<int, 0>{}, r);
+    for (int u = t; u < NU0 + NU1; u += NT) {
+      if (u < NU0)
+        face_run(std::integral_constant<int, 0>{}, u);
       else
-        face_item(std::integral_constant<int, 1>{}, r - B::V0N);
+        face_run(std::integral_constant<int, 1>{}, u - NU0);
     }
   }
   __syncthreads();
