@@ -510,7 +510,10 @@ def main():
     peak, peak_kind = load_peaks()
     tr = load_traffic()
     kernel = "batch_stage_kernel<2,float>"
-    traffic = tr.get(kernel, {}).get("dram_bytes_per_launch") if tr else None
+    # DRAM bytes per inner cell from the committed ncu capture, times this
+    # run's inner cells (traffic grows with the cells a launch processes)
+    per_cell = tr.get(kernel, {}).get("dram_bytes_per_inner_cell") if tr else None
+    traffic = per_cell * cells if per_cell else None
 
     cpu = None
     if ctx.rank == 0 and ctx.world == 1 and not a.no_cpu_baseline and not a.only_batched:
