@@ -42,7 +42,7 @@ class _Driver(ctypes.Structure):
 class _Grid(ctypes.Structure):
     _fields_ = [("ndim", _I), ("n", _I * 3), ("gamma", _D), ("chyp", _D * 13),
                 ("btype", _I * 3), ("g", _D * 3), ("courant", _D), ("hyperdif", _I),
-                ("delx", _PD * 3), ("drv", ctypes.POINTER(_Driver))]
+                ("delx", _PD * 3), ("drv", ctypes.POINTER(_Driver)), ("bmask", _I * 3), ("fixed", _PD)]
 
 
 class _State(ctypes.Structure):
@@ -96,6 +96,13 @@ class Oracle:
                 self.drv.xmin[d] = float(prob.xmin[d])
                 self.drv.dx[d] = float(prob.dx[d])
             g.drv = ctypes.pointer(self.drv)
+        bm = tuple(getattr(prob, "bmask", (0, 0, 0))) + (0, 0, 0)
+        for d in range(3):
+            g.bmask[d] = int(bm[d]) if d < prob.ndim else 0
+        # fixed boundaries keep the values of the state as loaded (captured
+        # before the initial ghost fill, as iosmaug.cpp:645-654 does at it=-1)
+        self.fixed = np.ascontiguousarray(prob.w, dtype=np.float64).copy()
+        g.fixed = _ptr(self.fixed)
         self.g = g
         self.s = _State()
         self.s.dt = 1.0e-8 if dt_fixed == 0.0 else dt_fixed
@@ -173,6 +180,14 @@ class Reference:
         bt = (_I * D)(*prob.btype)
         g = (_D * 3)(*(list(prob.g) + [0.0] * 3)[:3])
         L.ref_init(n, xmin, dx, prob.gamma, chyp, bt, prob.courant, 1, prob.hyperdif, 0.0, g)
+        # fields that take asymm on symm dims (the reference keeps a type per field)
+        bm = tuple(getattr(prob, "bmask", (0, 0, 0))) + (0, 0, 0)
+        nw = 2 + 2 * D
+        for d in range(D):
+            if prob.btype[d] == 6:
+                for f in range(nw):
+                    if (bm[d] >> f) & 1:
+                        L.ref_set_btype(f, d, 7)
         w = np.ascontiguousarray(prob.w)
         L.ref_set_state(_ptr(w))
         self.nstep = 0

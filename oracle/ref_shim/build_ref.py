@@ -28,6 +28,11 @@ Recipe (our own; the reference Makefile is not run):
    P2 computedervfields.cu:1353 -- ``temp[index]=0.0`` with ``index``
       uninitialised (undefined behaviour) becomes ``temp[iindex]=0.0``; those
       entries are already 0 at that point.
+   P4 boundary.cu -- the model file's cuboundary is renamed model_cuboundary
+      and bc_dispatch.inc (ours) becomes cuboundary: periodic and contcd4
+      still go to the model file, cont / fixed / symm / asymm to the
+      per-direction helpers of gradops.cu (the shipped model files each
+      implement a different subset of the boundary types).
    P3 boundary.cu -- models/boundary.cu.sedov3d (periodic, contcd4 and fixed
       ghosts, 2-D and 3-D; the file the Makefile's sedov3d target installs) is
       used for every model.  Its boundary0_per_parallel/boundary1_per_parallel
@@ -165,6 +170,11 @@ def transform(text: str, fname: str) -> str:
         out, n0 = re.subn(r"^kp=0;", "/* kp=0; removed by build_ref.py (P3) */", out, flags=re.M)
         if n0 != 2:
             raise RuntimeError(f"P3 patch expected 2 sites in boundary.cu.sedov3d, found {n0}")
+        # P4: the other boundary types through the gradops.cu helpers
+        out, n0 = re.subn(r"^int\s+cuboundary\s*\(", "int model_cuboundary(", out, flags=re.M)
+        if n0 != 1:
+            raise RuntimeError(f"P4 expected one cuboundary in boundary.cu.sedov3d, found {n0}")
+        out += '\n#include "bc_dispatch.inc"\n'
     if fname == "computedervfields.cu":
         n0 = out.count("temp[index]=0.0;")
         out = out.replace("temp[index]=0.0;", "temp[iindex]=0.0;")

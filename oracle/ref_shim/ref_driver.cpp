@@ -101,10 +101,27 @@ int ref_init(const int *n, const double *xmin, const double *dx, double gamma,
   return 0;
 }
 
+/* Boundary type of one field along one dim (both sides), after ref_init. */
+int ref_set_btype(int field, int dim, int type) {
+  if (field < 0 || field >= NVAR || dim < 0 || dim >= NDIM) return -1;
+  p->boundtype[field][dim][0] = p->boundtype[field][dim][1] = type;
+  d_p->boundtype[field][dim][0] = d_p->boundtype[field][dim][1] = type;
+  return 0;
+}
+
 /* w: NVAR*dimp, field-major, x fastest (the wmod slot layout, iotypes.h:213). */
 int ref_set_state(const double *w) {
   memcpy(d_wmod, w, sizeof(real) * NVAR * dimp);
   memcpy(d_wmod + (size_t)NVAR * dimp, w, sizeof(real) * NVAR * dimp);
+  /* iosmaug.cpp:645-654: fixed boundaries are captured from slot 0 at it = -1 */
+  const int its = p->it;
+  p->it = -1;
+  d_p->it = -1;
+  for (int ii = 0; ii < NVAR; ii++)
+    for (int idir = 0; idir < NDIM; idir++)
+      if (p->boundtype[ii][idir][0] == 5) cuboundary(&p, &bp, &d_p, &d_bp, &d_state, &d_wmod, 0, idir, ii);
+  p->it = its;
+  d_p->it = its;
   /* iosmaug.cpp:786-794: boundary on slot 1 for the evolved fields */
   for (int ii = 0; ii <= (b1 + (NDIM - 1)); ii++)
     for (int idir = 0; idir < NDIM; idir++)

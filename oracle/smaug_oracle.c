@@ -339,9 +339,41 @@ static void hyperviscosity(const sm_oracle_grid *g, const lay_t *L, const double
 
 /* ------------------------------------------------------------ boundaries */
 
-/* models/boundary.cu.sedov3d: boundary{0,1,2}_per_parallel (periodic) and
- * boundary{0,1,2}_contcd4_parallel, applied field by field and direction by
- * direction as iosmaug.cpp:1157-1166 calls cuboundary. */
+/* Ghost fill of the evolved fields, field by field and, for each field,
+ * direction by direction (iosmaug.cpp:1157-1166 calls cuboundary in that
+ * order), so a corner takes the rule of its last direction applied to the
+ * values the earlier directions left.  Per direction d, ghost x of n cells:
+ *   0 periodic  x <- x + (n-4) or x - (n-4)   (boundary.cu.sedov3d
+ *               boundary{0,1,2}_per_parallel)
+ *   3 cont      0,1 <- 2;  n-2,n-1 <- n-3     (gradops.cu:1043-1050,
+ *               bc3_cont_dir)
+ *   4 contcd4   0 <- 4, 1 <- 3, n-1 <- n-5, n-2 <- n-4
+ *               (boundary.cu.sedov3d boundary{0,1,2}_contcd4_parallel)
+ *   5 fixed     the values the state was loaded with (bc3_setfixed_dir at
+ *               it = -1, iosmaug.cpp:645-654, and bc3_fixed_dir,
+ *               gradops.cu:1201-1269).  The helper's tests read
+ *               `i==0 || i==1 && dir==0` (gradops.cu:1244-1257), so the pass
+ *               along d also restores the outermost ghost layer (0 and n-1)
+ *               of every earlier direction; reproduced.
+ *   6 symm      2-D: 0 <- 3, 1 <- 2, n-1 <- n-4, n-2 <- n-3;
+ *               3-D: 0 <- 4, 1 <- 3, n-1 <- n-5, n-2 <- n-4
+ *               (bc3_symm_dir, gradops.cu:1324-1395)
+ *   7 asymm     the symm source, negated (bc3_asymm_dir, gradops.cu:1396-1468);
+ *               also fields in bmask[d] where btype[d] is symm. */
+static int bsrc(int type, int D, int n, int x, double *sign) {
+  *sign = 1.0;
+  switch (type) {
+    case 0: return x < 2 ? x + (n - 4) : x - (n - 4);
+    case 3: return x < 2 ? 2 : n - 3;
+    case 4: return x == 0 ? 4 : x == 1 ? 3 : x == n - 1 ? n - 5 : n - 4;
+    case 7: *sign = -1.0; /* fall through */
+    case 6:
+      if (D == 2) return x == 0 ? 3 : x == 1 ? 2 : x == n - 1 ? n - 4 : n - 3;
+      return x == 0 ? 4 : x == 1 ? 3 : x == n - 1 ? n - 5 : n - 4;
+    default: return -1;
+  }
+}
+
 void sm_oracle_boundary(const sm_oracle_grid *g, double *w) {
   lay_t L0 = mklay(g);
   const lay_t *L = &L0;
@@ -350,23 +382,24 @@ void sm_oracle_boundary(const sm_oracle_grid *g, double *w) {
       double *a = F(w, f);
       const int n = L->n[d];
       const long s = L->st[d];
+      int type = g->btype[d];
+      if (type == 6 && ((g->bmask[d] >> f) & 1)) type = 7;
       for (long idx = 0; idx < L->N; ++idx) {
         int c[3];
         coords(L, idx, c);
         const int x = c[d];
-        if (g->btype[d] == 0) {
-          if (x == 0 || x == 1)
-            a[idx] = a[idx + (long)(n - 4) * s];
-          else if (x == n - 1 || x == n - 2)
-            a[idx] = a[idx + (long)(4 - n) * s];
-        } else if (g->btype[d] == 4) {
-          if (x == 0 || x == 1)
-            a[idx] = a[idx + (long)(4 - 2 * x) * s];
-          else if (x == n - 1)
-            a[idx] = a[idx - 4 * s];
-          else if (x == n - 2)
-            a[idx] = a[idx - 2 * s];
+        if (type == 5) {
+          int hit = !(x >= 2 && x <= n - 3);
+          for (int e = 0; e < d; ++e)
+            if (c[e] == 0 || c[e] == L->n[e] - 1) hit = 1;
+          if (hit && g->fixed) a[idx] = g->fixed[(long)f * L->N + idx];
+          continue;
         }
+        if (x >= 2 && x <= n - 3) continue;
+        double sign;
+        const int xs = bsrc(type, L->D, n, x, &sign);
+        if (xs < 0) continue;
+        a[idx] = sign * a[idx + (long)(xs - x) * s];
       }
     }
 }

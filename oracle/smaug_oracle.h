@@ -45,12 +45,15 @@ typedef struct {
   int n[3];            /* cells per dim incl. ghosts (n[2] = 1 in 2-D) */
   double gamma;
   double chyp[13];     /* hyperdiffusion coefficient per field id */
-  int btype[3];        /* per dim: 0 periodic, 4 contcd4 (iotypes.h:145) */
+  int btype[3];        /* per dim (iotypes.h:145): 0 periodic, 3 cont, 4 contcd4,
+                          5 fixed, 6 symm, 7 asymm */
   double g[3];         /* gravity per dim */
   double courant;
   int hyperdif;        /* 1: hyperdiffusion sources on (p->hyperdifmom) */
   const double *delx[3];
   const sm_oracle_driver *drv;  /* NULL: no driver */
+  int bmask[3];        /* per dim: evolved fields (bit f) that take asymm where btype is symm */
+  const double *fixed; /* fixed (5) boundaries: the state as loaded (NVAR * N), or NULL */
 } sm_oracle_grid;
 
 /* Per-run scalars carried between steps (p->dt, p->dtdiffvisc, p->maxviscoef). */
@@ -91,7 +94,9 @@ double sm_oracle_stage(const sm_oracle_grid *g, const double *win, const double 
 double sm_oracle_stage_t(const sm_oracle_grid *g, const double *win, const double *wbase,
                          double *wout, double h, const double *cmax, double tin);
 
-/* Ghost fill of the evolved fields (models/boundary.cu.sedov3d semantics). */
+/* Ghost fill of the evolved fields, field by field and direction by direction
+ * (iosmaug.cpp:1157-1166): periodic and contcd4 as models/boundary.cu.sedov3d,
+ * cont, fixed, symm and asymm as the per-direction helpers of src/gradops.cu. */
 void sm_oracle_boundary(const sm_oracle_grid *g, double *w);
 
 /*

@@ -48,7 +48,7 @@ class Problem:
     xmin: tuple         # coordinate of cell 0 (a ghost) per dim
     gamma: float
     chyp: np.ndarray    # per field id
-    btype: tuple        # per dim: 0 periodic, 4 contcd4
+    btype: tuple        # per dim: 0 periodic, 3 cont, 4 contcd4, 5 fixed, 6 symm, 7 asymm
     courant: float
     w: np.ndarray       # (NVAR, [n2,] n1, n0) float64
     g: tuple = (0.0, 0.0, 0.0)
@@ -56,6 +56,8 @@ class Problem:
     meta: dict = field(default_factory=dict)
     # momentum driver: {"dir", "amp", "period", "center", "width"} (None: off)
     driver: dict | None = None
+    # per dim: evolved fields (bit f) that take asymm where btype is symm
+    bmask: tuple = (0, 0, 0)
 
     @property
     def ncells(self) -> int:

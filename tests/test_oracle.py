@@ -42,7 +42,7 @@ def test_oracle_reproduces_golden(name):
     assert states_match(o.w, gold["w_final"], spec, meta["source"])
 
 
-def _run_ref_vs_oracle(kind, n, btype, steps):
+def _run_ref_vs_oracle(kind, n, btype, steps, bmask=None):
     code = f"""
 import sys, numpy as np
 sys.path.insert(0, {str(ROOT)!r}); sys.path.insert(0, {str(ROOT / 'smaug-all_b200' / 'python')!r})
@@ -50,6 +50,7 @@ from smaug_b200 import problems
 from oracle.oracle import Oracle, Reference
 prob = problems.orszag_tang({n}) if {kind!r} == 'ot' else problems.blast_wave({n}, seed=7)
 if {btype!r}: prob.btype = tuple({btype!r})
+if {bmask!r}: prob.bmask = tuple({bmask!r})
 r = Reference(prob); o = Oracle(prob)
 for s in range({steps}):
     wr = r.step(1); wo = o.step(1, rk4=False)
@@ -67,6 +68,29 @@ print('OK')
 ])
 def test_oracle_bit_exact_vs_reference_live(kind, n, btype, steps):
     _run_ref_vs_oracle(kind, n, btype, steps)
+
+
+# Boundary types beyond periodic / contcd4 (the reference's per-direction
+# helpers in src/gradops.cu, reached through the shim's boundary dispatch).
+# bmask: fields that take asymm on a symm dim (2-D: m_x = bit 1, m_y = bit 2,
+# B_x = bit 4, B_y = bit 5; 3-D: m = bits 1-3, B = bits 5-7).  3-D grids are
+# cubic and keep cont off the z direction: the reference's fixed-boundary
+# index helpers (gradops.cu:100-114) collide on other shapes, and its z branch
+# of bc3_cont_dir copies from (i, 2, k) instead of (i, j, 2) (gradops.cu:1005).
+BOUNDARY_CASES = [
+    ("ot", 24, [3, 3], 5, None), ("ot", 24, [5, 5], 5, None), ("ot", 24, [6, 6], 5, [0b10010, 0b100100]),
+    ("ot", 24, [7, 7], 4, None), ("ot", 24, [0, 5], 5, None), ("ot", 24, [5, 3], 5, None),
+    ("ot", 24, [6, 0], 5, None),
+    ("blast", 12, [3, 3, 0], 4, None), ("blast", 12, [5, 5, 5], 4, None),
+    ("blast", 12, [6, 6, 6], 4, [0b100010, 0b1000100, 0b10001000]), ("blast", 12, [7, 0, 6], 4, None),
+    ("blast", 12, [0, 3, 5], 4, None),
+]
+
+
+@pytest.mark.skipif(not all(p.exists() for p in REF_LIBS), reason="host build of the reference not present")
+@pytest.mark.parametrize("kind,n,btype,steps,bmask", BOUNDARY_CASES)
+def test_oracle_boundary_types_bit_exact_vs_reference(kind, n, btype, steps, bmask):
+    _run_ref_vs_oracle(kind, n, btype, steps, bmask)
 
 
 def test_metric_is_tensor_product_inside():
