@@ -52,8 +52,31 @@ enum {
   SMAUG_ERR_FULL = -5       /* batch: no free slot or arena block for a simulation */
 };
 
-/* Boundary types per direction (iotypes.h:145 boundtype codes). */
-enum { SMAUG_BC_PERIODIC = 0, SMAUG_BC_CONTCD4 = 4 };
+/*
+ * Boundary types per direction (iotypes.h:145 boundtype codes).  The ghosts
+ * are filled field by field, direction by direction (iosmaug.cpp:1157-1166):
+ *   PERIODIC  wrap (models/boundary.cu.sedov3d)
+ *   CONT      copies of the first/last inner cell (bc3_cont_dir, gradops.cu)
+ *   CONTCD4   0 <- 4, 1 <- 3, n-1 <- n-5, n-2 <- n-4 (boundary.cu.sedov3d)
+ *   FIXED     the values of the loaded state (bc3_setfixed_dir at it = -1,
+ *             bc3_fixed_dir; iosmaug.cpp:645-654); as in the reference, a
+ *             fixed direction also keeps the outermost ghost layer of every
+ *             earlier direction at its loaded values
+ *   SYMM      mirror (bc3_symm_dir; 2-D about the boundary face, 3-D about
+ *             the first inner cell, as the reference's 2-D and 3-D branches)
+ *   ASYMM     the mirror negated (bc3_asymm_dir)
+ * The reference keeps a type per field; here a type per direction applies to
+ * every evolved field, except that the fields in bmask[d] take ASYMM where
+ * btype[d] is SYMM (a reflecting wall: the normal momentum and field flip).
+ */
+enum {
+  SMAUG_BC_PERIODIC = 0,
+  SMAUG_BC_CONT = 3,
+  SMAUG_BC_CONTCD4 = 4,
+  SMAUG_BC_FIXED = 5,
+  SMAUG_BC_SYMM = 6,
+  SMAUG_BC_ASYMM = 7
+};
 
 /*
  * Arithmetic of the step.  The reference computes everything in FP64 (real =
@@ -74,7 +97,7 @@ typedef struct {
   double gamma;     /* p->gamma */
   double courant;   /* p->courant */
   double chyp[13];  /* p->chyp, indexed by field id (layout above) */
-  int btype[3];     /* per dim, SMAUG_BC_*; same for every field and both sides */
+  int btype[3];     /* per dim, SMAUG_BC_*; every evolved field, both sides (bmask below) */
   double g[3];      /* p->g */
   int hyperdif;     /* p->hyperdifmom: 1 = hyperdiffusion sources on */
   int rk4;          /* 1: classical four-stage RK (SAC fourstep); 0: single step (rkon=0) */
@@ -101,6 +124,8 @@ typedef struct {
   double drv_width[3];
   double xmin[3];         /* coordinate of cell 0 (a ghost) per dim */
   double dx[3];           /* grid spacing per dim */
+  int bmask[3];           /* per dim: evolved fields (bit = field id) that take
+                             SMAUG_BC_ASYMM where btype is SMAUG_BC_SYMM */
 } smaug_params;
 
 /* Number of fields for ndim (10 or 13). */

@@ -27,6 +27,8 @@
 namespace {
 
 constexpr int kGraphSteps = 16;  // steps per replay of the long graph
+// launches per step: dt, four stages each followed by its ghost pass, finish
+constexpr int kLaunchesPerStep = 10;
 
 __global__ void batch_dt_kernel(BatchInst *tab, long long *left, int *status, int n, int D) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -104,6 +106,9 @@ struct smaug_batch {
   std::vector<BatchInst> h_tab;
   std::vector<Slot> slots;
   WorkItem *d_work = nullptr;
+  WorkItem *d_gwork = nullptr;  // ghost chunks (256 ghost cells of one simulation each)
+  size_t gwork_cap = 0;
+  int ngwork = 0, ggrid = 0;
   size_t work_cap = 0;
   int nwork = 0, grid = 0, variant = 0, sms = 148;
   bool dirty = true;
@@ -175,13 +180,25 @@ void set_tiles(const smaug_batch *b, BatchInst &I) {
 // Rebuild the work list and the persistent grid for the current simulations
 // and tile shape.
 int rebuild(smaug_batch *b) {
-  std::vector<WorkItem> w;
+  std::vector<WorkItem> w, gw;
   for (int i = 0; i < b->max_inst; ++i) {
     if (!b->slots[i].used) continue;
     set_tiles(b, b->h_tab[i]);
     const int nt = b->h_tab[i].tiles[0] * b->h_tab[i].tiles[1] * b->h_tab[i].tiles[2];
     for (int t = 0; t < nt; ++t) w.push_back({i, t});
+    const long long ng = ghost_cells(b->h_tab[i].geo, b->D);
+    for (long long t = 0; t < (ng + 255) / 256; ++t) gw.push_back({i, (int)t});
   }
+  if (gw.size() > b->gwork_cap) {
+    BK(cudaStreamSynchronize(b->stream));
+    if (b->d_gwork) cudaFree(b->d_gwork);
+    b->gwork_cap = std::max(gw.size(), (size_t)1024) * 2;
+    BK(cudaMalloc(&b->d_gwork, sizeof(WorkItem) * b->gwork_cap));
+  }
+  if (!gw.empty())
+    BK(cudaMemcpyAsync(b->d_gwork, gw.data(), sizeof(WorkItem) * gw.size(), cudaMemcpyHostToDevice, b->stream));
+  b->ngwork = (int)gw.size();
+  b->ggrid = std::min(b->ngwork, 148 * 8);
   BK(cudaMemcpyAsync(b->d_tab, b->h_tab.data(), sizeof(BatchInst) * b->max_inst, cudaMemcpyHostToDevice, b->stream));
   if (w.size() > b->work_cap) {
     BK(cudaStreamSynchronize(b->stream));
@@ -220,6 +237,7 @@ void enqueue_step(smaug_batch *b, cudaStream_t s, bool timed = false) {
     }
     smaug_batchk::launch_batch_stage(b->D, b->mixed, b->variant, b->d_tab, b->d_work, b->nwork, k, b->grid, s);
     if (e1) cudaEventRecord(e1, s);
+    smaug_batchk::launch_batch_ghost(b->D, b->mixed, b->d_tab, b->d_gwork, b->ngwork, k, b->ggrid, s);
   }
   batch_finish_kernel<<<nb, 128, 0, s>>>(b->d_tab, b->d_status, b->max_inst);
 }
@@ -294,6 +312,7 @@ int smaug_batch_destroy(smaug_batch *b) {
   cudaFree(b->d_left);
   cudaFree(b->d_status);
   cudaFree(b->d_work);
+  cudaFree(b->d_gwork);
   if (b->stream) cudaStreamDestroy(b->stream);
   if (b->cap) cudaStreamDestroy(b->cap);
   delete b;
@@ -377,13 +396,24 @@ int smaug_batch_add(smaug_batch *b, const smaug_params *prm, const double *delx,
   BK(cudaMemcpyAsync(dxlast, delx + (size_t)(p.D - 1) * N, sizeof(double) * N, cudaMemcpyHostToDevice, s));
   BK(cudaMemcpyAsync(I.W[0], w, sizeof(double) * p.NW * N, cudaMemcpyHostToDevice, s));
   BK(cudaMemcpyAsync(bg, bh, sizeof(double) * p.NB * N, cudaMemcpyHostToDevice, s));
-  ghost_fill_kernel<<<148 * 8, 256, 0, s>>>(I.W[0], p.NW, p.geo, p.D);
+  ghost_fill(I.W[0], p.NW, p.geo, p.D, s);
   const double dt0 = p.phys.dt_mode == 1 ? (p.dt0 > 0 ? p.dt0 : 1.0e-8) : p.dt0;
   one_reset_kernel<<<1, 1, 0, s>>>(sc, dt0);
-  smaug_fast::launch_reduce(p.D, I.W[0], bg, p.geo, p.phys, &sc->red[0], s);
+  smaug_fast::launch_reduce(p.D, I.W[0], bg, p.geo, p.phys, &sc->red[0], s, 0);
+  if (p.geo.has_const) smaug_fast::launch_reduce(p.D, I.W[0], bg, p.geo, p.phys, &sc->floor, s, 1);
   if (p.mixed) split_kernel<<<148 * 8, 256, 0, s>>>(I.W[0], I.F[0], I.F[1], (long long)p.NW * N);
-  b->launches += p.mixed ? 4 : 3;
+  b->launches += p.D + 2 + (p.mixed ? 1 : 0) + (p.geo.has_const ? 1 : 0);
   BK(cudaGetLastError());
+  if (p.geo.has_const) {  // fixed boundaries: every stage buffer holds the loaded ghosts
+    const size_t n = (size_t)p.NW * N;
+    if (p.mixed) {
+      for (int k = 2; k < 4; ++k)
+        BK(cudaMemcpyAsync(I.F[k], I.F[0], sizeof(float) * n, cudaMemcpyDeviceToDevice, s));
+    } else {
+      for (int k = 1; k < 4; ++k)
+        BK(cudaMemcpyAsync(I.W[k], I.W[0], sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
+    }
+  }
   BK(cudaMemcpyAsync(b->d_left + slot, &nsteps, sizeof(long long), cudaMemcpyHostToDevice, s));
   const int zero = 0;
   BK(cudaMemcpyAsync(b->d_status + slot, &zero, sizeof(int), cudaMemcpyHostToDevice, s));
@@ -422,7 +452,7 @@ int smaug_batch_step(smaug_batch *b, int nsteps) {
   if (b->nwork == 0) return SMAUG_OK;
   if (b->profile) {
     for (int i = 0; i < nsteps; ++i) enqueue_step(b, b->stream, true);
-    b->launches += 6LL * nsteps;
+    b->launches += (long long)kLaunchesPerStep * nsteps;
     BK(cudaGetLastError());
     return SMAUG_OK;
   }
@@ -436,11 +466,11 @@ int smaug_batch_step(smaug_batch *b, int nsteps) {
   }
   for (int i = 0; i + kGraphSteps <= nsteps; i += kGraphSteps) {
     BK(cudaGraphLaunch(b->gk, b->stream));
-    b->launches += 6LL * kGraphSteps;
+    b->launches += (long long)kLaunchesPerStep * kGraphSteps;
   }
   for (int i = 0; i < nsteps % kGraphSteps; ++i) {
     BK(cudaGraphLaunch(b->g1, b->stream));
-    b->launches += 6;
+    b->launches += kLaunchesPerStep;
   }
   return SMAUG_OK;
 }

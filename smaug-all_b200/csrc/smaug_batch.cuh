@@ -82,6 +82,10 @@ void launch_batch_stage_2f(int, const smaug::BatchInst *, const smaug::WorkItem 
 void launch_batch_stage_2d(int, const smaug::BatchInst *, const smaug::WorkItem *, int, int, int, cudaStream_t);
 void launch_batch_stage_3f(int, const smaug::BatchInst *, const smaug::WorkItem *, int, int, int, cudaStream_t);
 void launch_batch_stage_3d(int, const smaug::BatchInst *, const smaug::WorkItem *, int, int, int, cudaStream_t);
+void launch_batch_ghost_2f(const smaug::BatchInst *, const smaug::WorkItem *, int, int, int, cudaStream_t);
+void launch_batch_ghost_2d(const smaug::BatchInst *, const smaug::WorkItem *, int, int, int, cudaStream_t);
+void launch_batch_ghost_3f(const smaug::BatchInst *, const smaug::WorkItem *, int, int, int, cudaStream_t);
+void launch_batch_ghost_3d(const smaug::BatchInst *, const smaug::WorkItem *, int, int, int, cudaStream_t);
 int batch_stage_occupancy_2f(int);
 int batch_stage_occupancy_2d(int);
 int batch_stage_occupancy_3f(int);
@@ -96,6 +100,15 @@ inline void launch_batch_stage(int D, bool mixed, int variant, const smaug::Batc
     (mixed ? launch_batch_stage_2f : launch_batch_stage_2d)(variant, tab, work, nwork, stage, grid, st);
   else
     (mixed ? launch_batch_stage_3f : launch_batch_stage_3d)(variant, tab, work, nwork, stage, grid, st);
+}
+// The ghost pass of RK stage `stage` (gwork == nullptr: the n chunks of
+// simulation 0).
+inline void launch_batch_ghost(int D, bool mixed, const smaug::BatchInst *tab, const smaug::WorkItem *gwork, int n,
+                               int stage, int grid, cudaStream_t st) {
+  if (D == 2)
+    (mixed ? launch_batch_ghost_2f : launch_batch_ghost_2d)(tab, gwork, n, stage, grid, st);
+  else
+    (mixed ? launch_batch_ghost_3f : launch_batch_ghost_3d)(tab, gwork, n, stage, grid, st);
 }
 // Blocks per SM the stage kernel of (D, mixed, variant) can keep resident.
 inline int batch_stage_occupancy(int D, bool mixed, int variant) {

@@ -95,6 +95,7 @@ void launch_stage(Run &r, const StageArgs &a) {
     else
       smaug_fast::launch_stage(r.D, r.mixed, a, r.geo, r.phys, r.stream);
   });
+  if (!r.exact) r.launches++;  // the tiled build's ghost pass
 }
 
 // RK stage k (1..4) of the production path: the batch stage kernel, one
@@ -104,6 +105,10 @@ void launch_rk_stage(Run &r, int k) {
     smaug_batchk::launch_batch_stage(r.D, r.mixed, batch_default_variant(r.D, r.mixed), r.inst, nullptr, r.ntiles, k,
                                      r.ntiles, r.stream);
   });
+  // its ghost pass: the ghost chunks of this simulation
+  const int nch = (int)((ghost_cells(r.geo, r.D) + 255) / 256);
+  smaug_batchk::launch_batch_ghost(r.D, r.mixed, r.inst, nullptr, nch, k, std::min(nch, 148 * 8), r.stream);
+  r.launches++;
 }
 
 // Describe the simulation to the batch stage kernel (production RK4 path).
@@ -131,20 +136,37 @@ cudaError_t run_upload_inst(Run &r) {
 
 // A state is in r.W[0] (evolved) and r.bg: fill ghosts, reset scalars,
 // reduce the initial maxima (and, mixed, split it into value +
-// compensation).  Asynchronous.
+// compensation).  With fixed boundaries the maxima of the cells that keep
+// their loaded values become the floor of every step's maxima, and every
+// stage buffer gets those cells.  Asynchronous.
 cudaError_t run_load(Run &r) {
   r.cur = 0;
-  ghost_fill_kernel<<<148 * 8, 256, 0, r.stream>>>(r.W[0], r.NW, r.geo, r.D);
+  ghost_fill(r.W[0], r.NW, r.geo, r.D, r.stream);
   const double dt0 = r.phys.dt_mode == 1 ? (r.dt0 > 0 ? r.dt0 : 1.0e-8) : r.dt0;
   reset_scalars_kernel<<<1, 1, 0, r.stream>>>(r.sc, dt0);
-  if (r.exact)
-    smaug_exact::launch_reduce(r.D, r.W[0], r.bg, r.geo, r.phys, &r.sc->red[0], r.stream);
-  else
-    smaug_fast::launch_reduce(r.D, r.W[0], r.bg, r.geo, r.phys, &r.sc->red[0], r.stream);
-  r.launches += 3;
+  auto reduce = r.exact ? smaug_exact::launch_reduce : smaug_fast::launch_reduce;
+  reduce(r.D, r.W[0], r.bg, r.geo, r.phys, &r.sc->red[0], r.stream, 0);
+  r.launches += r.D + 2;
+  if (r.geo.has_const) {
+    reduce(r.D, r.W[0], r.bg, r.geo, r.phys, &r.sc->floor, r.stream, 1);
+    r.launches++;
+  }
   if (r.mixed) {
     split_kernel<<<148 * 8, 256, 0, r.stream>>>(r.W[0], r.F[0], r.F[1], (long long)r.NW * r.geo.N);
     r.launches++;
+  }
+  if (r.geo.has_const) {
+    const size_t n = (size_t)r.NW * r.geo.N;
+    for (int k = 1; k < 4; ++k)
+      if (!r.mixed && r.W[k]) {
+        const cudaError_t e = cudaMemcpyAsync(r.W[k], r.W[0], sizeof(double) * n, cudaMemcpyDeviceToDevice, r.stream);
+        if (e != cudaSuccess) return e;
+      }
+    if (r.mixed)
+      for (int k = 2; k < 4; ++k) {
+        const cudaError_t e = cudaMemcpyAsync(r.F[k], r.F[0], sizeof(float) * n, cudaMemcpyDeviceToDevice, r.stream);
+        if (e != cudaSuccess) return e;
+      }
   }
   return cudaGetLastError();
 }

@@ -14,13 +14,13 @@ namespace smaug_exact {
 void launch_stage(int D, bool mixed, const smaug::StageArgs &a, const smaug::Geo &g, const smaug::Phys &p,
                   cudaStream_t st);
 void launch_reduce(int D, const double *w, const double *bg, const smaug::Geo &g, const smaug::Phys &p,
-                   smaug::Reduce *r, cudaStream_t st);
+                   smaug::Reduce *r, cudaStream_t st, int const_only = 0);
 }  // namespace smaug_exact
 namespace smaug_fast {
 void launch_stage(int D, bool mixed, const smaug::StageArgs &a, const smaug::Geo &g, const smaug::Phys &p,
                   cudaStream_t st);
 void launch_reduce(int D, const double *w, const double *bg, const smaug::Geo &g, const smaug::Phys &p,
-                   smaug::Reduce *r, cudaStream_t st);
+                   smaug::Reduce *r, cudaStream_t st, int const_only = 0);
 }  // namespace smaug_fast
 
 using namespace smaug;
@@ -59,11 +59,23 @@ const char *plan_sim(const smaug_params *prm, SimPlan &r) {
   for (int d = 0; d < 3; ++d) {
     const int n = d < D ? prm->n[d] : 1;
     if (d < D && (n < 10 || n > (1 << 20))) return "each dimension needs 10..2^20 cells including ghosts";
-    if (d < D && prm->btype[d] != SMAUG_BC_PERIODIC && prm->btype[d] != SMAUG_BC_CONTCD4)
-      return "boundary type must be periodic (0) or contcd4 (4)";
+    if (d < D) {
+      const int t = prm->btype[d];
+      if (t != BC_PERIODIC && t != BC_CONT && t != BC_CONTCD4 && t != BC_FIXED && t != BC_SYMM && t != BC_ASYMM)
+        return "boundary type must be periodic (0), cont (3), contcd4 (4), fixed (5), symm (6) or asymm (7)";
+      if (prm->bmask[d] & ~((1 << (2 + 2 * D)) - 1)) return "bmask may name evolved fields only";
+    }
     r.geo.n[d] = n;
     r.geo.btype[d] = d < D ? prm->btype[d] : 0;
+    r.geo.bmask[d] = d < D ? prm->bmask[d] : 0;
     N *= n;
+  }
+  r.geo.has_const = 0;
+  for (int d = 0; d < 3; ++d) {
+    r.geo.outer_frozen[d] = 0;
+    for (int q = d + 1; q < D; ++q)
+      if (r.geo.btype[q] == BC_FIXED) r.geo.outer_frozen[d] = d < D;
+    if (d < D && r.geo.btype[d] == BC_FIXED) r.geo.has_const = 1;
   }
   if (N * (long long)r.NVAR >= (1LL << 31)) return "grid too large: NVAR * N must stay below 2^31";
   r.geo.st[0] = 1;
@@ -103,31 +115,38 @@ const char *plan_sim(const smaug_params *prm, SimPlan &r) {
   return nullptr;
 }
 
-// Ghost fill of the evolved fields from their interior sources (periodic /
-// contcd4), used when a state is loaded (iosmaug.cpp:786-794).
-__global__ void ghost_fill_kernel(double *w, int nw, Geo g, int D) {
+// One direction's pass of the ghost fill of the evolved fields (the rules of
+// smaug_device.cuh, field by field, direction by direction as
+// iosmaug.cpp:1157-1166): the ghost layers of d from their sources along d,
+// which this pass does not write.  Fixed layers, and outermost layers that a
+// later fixed pass restores, keep their values.
+__global__ void ghost_pass_kernel(double *w, int nw, Geo g, int D, int d) {
+  const int n = g.n[d], t = g.btype[d];
+  const unsigned neg = bc_neg(g, d);
   for (long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x; j < g.N; j += (long long)gridDim.x * blockDim.x) {
-    long long r = j;
-    int c[3] = {0, 0, 0};
-    c[0] = (int)(r % g.n[0]);
-    r /= g.n[0];
-    c[1] = (int)(r % g.n[1]);
-    c[2] = (int)(r / g.n[1]);
-    int s[3] = {c[0], c[1], c[2]};
-    bool ghost = false;
-    for (int d = 0; d < D; ++d) {
-      const int n = g.n[d], x = c[d];
-      if (x >= 2 && x <= n - 3) continue;
-      ghost = true;
-      if (g.btype[d] == 0)
-        s[d] = x < 2 ? x + (n - 4) : x - (n - 4);
-      else
-        s[d] = x == 0 ? 4 : x == 1 ? 3 : x == n - 1 ? n - 5 : n - 4;
+    const int x = (int)((j / g.st[d]) % n);
+    if (x >= 2 && x <= n - 3) continue;
+    if (t == BC_FIXED || (g.outer_frozen[d] && (x == 0 || x == n - 1))) continue;
+    const int xs = bc_source(t, D, n, x);
+    const long long src = j + (long long)(xs - x) * g.st[d];
+    for (int f = 0; f < nw; ++f) {
+      const double v = w[(long long)f * g.N + src];
+      w[(long long)f * g.N + j] = ((neg >> f) & 1u) ? -v : v;
     }
-    if (!ghost) continue;
-    const long long src = s[0] + (long long)s[1] * g.st[1] + (long long)s[2] * g.st[2];
-    for (int f = 0; f < nw; ++f) w[(long long)f * g.N + j] = w[(long long)f * g.N + src];
   }
+}
+
+// Ghost cells of a grid (a coordinate outside [2, n-3]).
+inline long long ghost_cells(const Geo &g, int D) {
+  long long in = 1;
+  for (int d = 0; d < D; ++d) in *= g.n[d] - 4;
+  return g.N - in;
+}
+
+// The ghost fill of a loaded state, used when a state is loaded
+// (iosmaug.cpp:786-794).
+void ghost_fill(double *w, int nw, const Geo &g, int D, cudaStream_t s) {
+  for (int d = 0; d < D; ++d) ghost_pass_kernel<<<148 * 8, 256, 0, s>>>(w, nw, g, D, d);
 }
 
 // The moddton dt block of the reference loop (iosmaug.cpp:855-898):
@@ -157,8 +176,7 @@ __device__ __forceinline__ void dt_update(DevScalars *sc, const Phys &p, int D) 
     if ((sc->dtdiffvisc) > 1.0e-8 && (sc->dt) > ((sc->dtdiffvisc))) sc->dt = sc->dtdiffvisc;
   }
   if (!isfinite(sc->dt) || sc->dt <= 0.0) sc->status = SMAUG_ERR_NONFINITE;
-  for (int s = 1; s < 5; ++s)
-    for (int k = 0; k < 8; ++k) sc->red[s].v[k] = 0ull;
+  for (int s = 1; s < 5; ++s) sc->red[s] = sc->floor;
 }
 
 // End of step: running maximum of the hyperviscosity (the reference's reset
@@ -188,6 +206,7 @@ __device__ __forceinline__ void reset_update(DevScalars *sc, double dt0) {
   sc->status = 0;
   for (int s = 0; s < 5; ++s)
     for (int k = 0; k < 8; ++k) sc->red[s].v[k] = 0ull;
+  for (int k = 0; k < 8; ++k) sc->floor.v[k] = 0ull;
 }
 
 // FP64 state -> FP32 value + FP32 compensation (w = hi + lo to ~48 bits).

@@ -40,13 +40,20 @@ struct DevScalars {
   int pad_;
   double t;       // simulation time at the start of the current step (driver)
   Reduce red[5];  // [0] state at step start, [1..3] RK stage outputs, [4] state at step end
+  // maxima over the ghost cells that keep their loaded values (fixed
+  // boundaries): the stage kernels never rewrite those cells, so each step's
+  // stage maxima start from these
+  Reduce floor;
 };
 
 struct Geo {
   int n[3];
   long long st[3];
   long long N;
-  int btype[3];
+  int btype[3];               // per dim: 0 periodic, 3 cont, 4 contcd4, 5 fixed, 6 symm, 7 asymm
+  int bmask[3];               // per dim: evolved fields (bit f) that take asymm where btype is symm
+  int outer_frozen[3];        // 1: a later dim is fixed, so the outermost ghost layer keeps its loaded values
+  int has_const;              // some ghost cells keep their loaded values (a fixed dim)
   long long K;                // courant cells below K are excluded from the viscous-dt maximum
   const double *dx1[3];       // metric along d at inner cells (depends on c_d only)
   const double *dxlast;       // full per-cell metric of the last dim (courant reduction)
@@ -284,6 +291,69 @@ __device__ __forceinline__ double driver_vvz(const Geo &g, const Phys &p, const 
   double tdep = 1.0;
   if (p.drv_period > 0.0) tdep = sin(2.0 * 3.14159265358979323846 * (sc->t + tfrac * sc->dt) / p.drv_period);
   return p.drv_amp * f * tdep;
+}
+
+// ------------------------------------------------------------- boundaries
+// The reference fills the ghosts field by field and, per field, direction by
+// direction (iosmaug.cpp:1157-1166).  The rule of one direction takes ghost
+// coordinate x of n cells from the source coordinate below, along the same
+// direction, so corners compose the rules in direction order:
+//   0 periodic  x +- (n-4)              (models/boundary.cu.sedov3d)
+//   3 cont      0,1 <- 2;  n-2,n-1 <- n-3   (bc3_cont_dir, gradops.cu:1043-1050)
+//   4 contcd4   0 <- 4, 1 <- 3, n-1 <- n-5, n-2 <- n-4   (boundary.cu.sedov3d)
+//   5 fixed     the loaded values (bc3_setfixed_dir / bc3_fixed_dir,
+//               gradops.cu:1201-1269); its tests read `i==0 || i==1 && dir==0`,
+//               so the pass also restores the outermost layer (0, n-1) of
+//               every earlier direction
+//   6 symm      2-D 0 <- 3, 1 <- 2, n-1 <- n-4, n-2 <- n-3; 3-D as contcd4
+//               (bc3_symm_dir, gradops.cu:1324-1395)
+//   7 asymm     the symm source negated (bc3_asymm_dir); on a symm direction
+//               the fields of bmask take this rule
+enum { BC_PERIODIC = 0, BC_CONT = 3, BC_CONTCD4 = 4, BC_FIXED = 5, BC_SYMM = 6, BC_ASYMM = 7 };
+
+// Source coordinate of ghost coordinate x along a direction of n cells (-1:
+// none, the fixed type).
+__host__ __device__ inline int bc_source(int type, int D, int n, int x) {
+  switch (type) {
+    case BC_PERIODIC: return x < 2 ? x + (n - 4) : x - (n - 4);
+    case BC_CONT: return x < 2 ? 2 : n - 3;
+    case BC_CONTCD4: return x == 0 ? 4 : x == 1 ? 3 : x == n - 1 ? n - 5 : n - 4;
+    case BC_SYMM:
+    case BC_ASYMM:
+      if (D == 2) return x == 0 ? 3 : x == 1 ? 2 : x == n - 1 ? n - 4 : n - 3;
+      return x == 0 ? 4 : x == 1 ? 3 : x == n - 1 ? n - 5 : n - 4;
+    default: return -1;
+  }
+}
+
+// Evolved fields (bit f) negated by the rule along d.
+__host__ __device__ inline unsigned bc_neg(const Geo &g, int d) {
+  return g.btype[d] == BC_ASYMM ? 0xffu : g.btype[d] == BC_SYMM ? (unsigned)g.bmask[d] : 0u;
+}
+
+// Does cell c keep its loaded value under the fill passes?  Walks back from
+// the last pass that writes the cell: a fixed pass restores it; another rule
+// moves to its source along that direction and continues with the earlier
+// passes; an inner cell evolves.
+template <int D>
+__host__ __device__ inline bool is_const_cell(const Geo &g, const int *c0) {
+  int c[3] = {c0[0], c0[1], c0[2]};
+  int limit = D - 1;
+  while (limit >= 0) {
+    int L = -1;
+    for (int q = limit; q >= 0 && L < 0; --q) {
+      bool covers = c[q] < 2 || c[q] > g.n[q] - 3;
+      if (!covers && g.btype[q] == BC_FIXED)
+        for (int e = 0; e < q; ++e)
+          if (c[e] == 0 || c[e] == g.n[e] - 1) covers = true;
+      if (covers) L = q;
+    }
+    if (L < 0) return false;
+    if (g.btype[L] == BC_FIXED) return true;
+    c[L] = bc_source(g.btype[L], D, g.n[L], c[L]);
+    limit = L - 1;
+  }
+  return false;
 }
 
 }  // namespace smaug

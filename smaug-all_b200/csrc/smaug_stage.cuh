@@ -70,23 +70,71 @@ __device__ __forceinline__ void block_max_flush(const float *v, Reduce *r) {
   block_max_flush<NV>(w, r);
 }
 
-// Coordinates along d that receive the value of inner coordinate x: x itself
-// plus its ghost image (periodic wrap, boundary{0,1,2}_per_parallel; or the
-// contcd4 copies 0<-4, 1<-3, n-1<-n-5, n-2<-n-4, boundary{0,1,2}_contcd4_parallel
-// of models/boundary.cu.sedov3d).  Returns the count (1 or 2).
-__device__ __forceinline__ int images(const Geo &g, int d, int x, int *xs) {
+// Coordinates along d that take the value of inner coordinate x once the
+// ghosts are filled (the per-direction rules above, applied in direction
+// order): xs[0] = x itself, then its ghost images (cont gives two); *neg =
+// the evolved fields the images take negated.  A fixed direction has no
+// images (its ghosts keep their loaded values), and where a later direction
+// is fixed the outermost layer is restored by that pass, so it is no image
+// either.  Returns the count (1..3).
+template <int D>
+__device__ __forceinline__ int images(const Geo &g, int d, int x, int *xs, unsigned *neg) {
+  // (fixed slots, no runtime index: the arrays stay in registers)
   const int n = g.n[d];
-  xs[0] = x;
-  if (g.btype[d] == 0) {
-    if (x == n - 4 || x == n - 3) { xs[1] = x - (n - 4); return 2; }
-    if (x == 2 || x == 3) { xs[1] = x + (n - 4); return 2; }
-  } else {
-    if (x == 4) { xs[1] = 0; return 2; }
-    if (x == 3) { xs[1] = 1; return 2; }
-    if (x == n - 5) { xs[1] = n - 1; return 2; }
-    if (x == n - 4) { xs[1] = n - 2; return 2; }
+  int k = 1, e1 = 0, e2 = 0;
+  switch (g.btype[d]) {
+    case BC_PERIODIC:
+      if (x == n - 4 || x == n - 3) {
+        e1 = x - (n - 4);
+        k = 2;
+      } else if (x == 2 || x == 3) {
+        e1 = x + (n - 4);
+        k = 2;
+      }
+      break;
+    case BC_CONT:
+      if (x == 2) {
+        e1 = 0;
+        e2 = 1;
+        k = 3;
+      } else if (x == n - 3) {
+        e1 = n - 1;
+        e2 = n - 2;
+        k = 3;
+      }
+      break;
+    case BC_SYMM:
+    case BC_ASYMM:
+      if (D == 2) {
+        k = 2;
+        if (x == 3) e1 = 0;
+        else if (x == 2) e1 = 1;
+        else if (x == n - 4) e1 = n - 1;
+        else if (x == n - 3) e1 = n - 2;
+        else k = 1;
+        break;
+      }
+      // fall through: the 3-D mirror is contcd4's
+    case BC_CONTCD4:
+      k = 2;
+      if (x == 4) e1 = 0;
+      else if (x == 3) e1 = 1;
+      else if (x == n - 5) e1 = n - 1;
+      else if (x == n - 4) e1 = n - 2;
+      else k = 1;
+      break;
+    default:
+      break;
   }
-  return 1;
+  if (g.outer_frozen[d] && k > 1 && (e1 == 0 || e1 == n - 1)) {  // drop images 0 and n-1
+    e1 = e2;
+    k -= 1;
+  }
+  xs[0] = x;
+  xs[1] = e1;
+  xs[2] = e2;
+  *neg = bc_neg(g, d);
+  return k;
 }
 
 // cfast/courant maxima of the state `o` written at cell idx (with that cell's
@@ -338,38 +386,49 @@ __global__ void __launch_bounds__(kBX *kBY) stage_kernel(StageArgs a, Geo g, Phy
     }
 
     // ---- write the cell and its ghost images, reduce wave speeds
-    int xs[3][2], nx[3];
+    int xs[3][3], nx[3];
+    unsigned ng[3];
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
       if (d < D)
-        nx[d] = images(g, d, c[d], xs[d]);
+        nx[d] = images<D>(g, d, c[d], xs[d], &ng[d]);
       else {
         nx[d] = 1;
         xs[d][0] = 0;
+        ng[d] = 0;
       }
     }
     for (int iz = 0; iz < nx[2]; ++iz)
       for (int iy = 0; iy < nx[1]; ++iy)
         for (int ix = 0; ix < nx[0]; ++ix) {
           const long long j = xs[0][ix] + (long long)xs[1][iy] * g.st[1] + (D == 3 ? (long long)xs[2][iz] * g.st[2] : 0);
+          const unsigned neg = (ix ? ng[0] : 0u) ^ (iy ? ng[1] : 0u) ^ (iz ? ng[2] : 0u);
+          double ov[NW];
 #pragma unroll
-          for (int f = 0; f < NW; ++f) a.out[(long long)f * N + j] = o[f];
+          for (int f = 0; f < NW; ++f) ov[f] = ((neg >> f) & 1u) ? -o[f] : o[f];
+#pragma unroll
+          for (int f = 0; f < NW; ++f) a.out[(long long)f * N + j] = ov[f];
           double bgv[NB];
 #pragma unroll
           for (int b = 0; b < NB; ++b) bgv[b] = __ldg(a.bg + (long long)b * N + j);
-          reduce_cell<D>(g, p, o, bgv, j, red);
+          reduce_cell<D>(g, p, ov, bgv, j, red);
         }
   }
   block_max_flush<6>(red, &a.sc->red[a.red_out]);
 }
 
-// Maxima over all cells of a state (used once after the state is loaded).
+// Maxima over all cells of a state (used once after the state is loaded);
+// const_only: over the cells that keep their loaded values only.
 template <int D>
-__global__ void reduce_state_kernel(const double *w, const double *bg, Geo g, Phys p, Reduce *r) {
+__global__ void reduce_state_kernel(const double *w, const double *bg, Geo g, Phys p, Reduce *r, int const_only) {
   using L = Lay<D>;
   constexpr int NW = L::NW, NB = L::NVAR - L::NW;
   double red[6] = {0, 0, 0, 0, 0, 0};
   for (long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x; j < g.N; j += (long long)gridDim.x * blockDim.x) {
+    if (const_only) {
+      const int c[3] = {(int)(j % g.n[0]), (int)((j / g.n[0]) % g.n[1]), (int)(j / g.st[2])};
+      if (!is_const_cell<D>(g, c)) continue;
+    }
     double o[NW], bgv[NB];
 #pragma unroll
     for (int f = 0; f < NW; ++f) o[f] = w[(long long)f * g.N + j];

@@ -221,8 +221,8 @@ __device__ __forceinline__ void reduce_cell_mixed(const Geo &g, const Phys &p, c
 }
 
 // The end of a stage for one cell: the stage output base + h dL with the
-// driver, the RK combination of the stage, the writes of the cell and its
-// ghost images, and the wave-speed / viscosity maxima, taken into the
+// driver, the RK combination of the stage, the write of the cell and the
+// wave-speed / viscosity maxima, taken into the
 // thread's running maxima red[6] (in the stencil type: FP32 values in the
 // mixed path; the caller flushes them to the simulation's reduction slot).
 template <int D, typename T>
@@ -290,28 +290,10 @@ __device__ __forceinline__ void stage_epilogue(const StageArgs &a, const Geo &g,
         o[f] = (double)hi[f];  // what the next stage reads
       }
     }
-    // the cell and its ghost images: per dim the own coordinate and, at most,
-    // one image coordinate (images()), combined over all dims
-    int x0[3], x1[3], has[3];
-#pragma unroll
-    for (int d = 0; d < 3; ++d) {
-      int xs[2] = {0, 0};
-      has[d] = d < D ? (images(g, d, c[d], xs) == 2) : 0;
-      x0[d] = d < D ? c[d] : 0;
-      x1[d] = xs[1];
-    }
-#pragma unroll
-    for (int m = 0; m < (1 << D); ++m) {
-      bool ok = true;
-      int cc[3];
-#pragma unroll
-      for (int d = 0; d < 3; ++d) {
-        const bool b = d < D && ((m >> d) & 1);
-        if (b && !has[d]) ok = false;
-        cc[d] = b ? x1[d] : x0[d];
-      }
-      if (!ok) continue;
-      const long long j = gidx<D>(g, cc);
+    // the cell (its ghost images are written by the ghost pass that follows
+    // every stage: ghost_cell below)
+    {
+      const unsigned j = (unsigned)idx;
       if (!MIXED) {
 #pragma unroll
         for (int f = 0; f < NW; ++f) a.out[fo32(f, g.N, j)] = o[f];
@@ -325,18 +307,155 @@ __device__ __forceinline__ void stage_epilogue(const StageArgs &a, const Geo &g,
 #pragma unroll
         for (int f = 0; f < NW; ++f) a.out32[fo32(f, g.N, j)] = hi[f];
       }
-      // backgrounds (e_b and B_b are zero everywhere without an energy
-      // background: only rho_b is read then)
-      double bgv[NB];
+    }
+    // backgrounds (e_b and B_b are zero everywhere without an energy
+    // background: only rho_b is read then), then the maxima
+    double bgv[NB];
 #pragma unroll
-      for (int b = 0; b < NB; ++b)
-        bgv[b] = (b == L::RHOB - NW || p.has_bgb) ? __ldg(a.bg + fo32(b, g.N, j)) : 0.0;
-      if constexpr (MIXED)
-        reduce_cell_mixed<D>(g, p, o, bgv, j, red);
-      else
-        reduce_cell<D>(g, p, o, bgv, j, red);
+    for (int b = 0; b < NB; ++b)
+      bgv[b] = (b == L::RHOB - NW || p.has_bgb) ? __ldg(a.bg + fo32(b, g.N, (unsigned)idx)) : 0.0;
+    if constexpr (MIXED)
+      reduce_cell_mixed<D>(g, p, o, bgv, idx, red);
+    else
+      reduce_cell<D>(g, p, o, bgv, idx, red);
+  }
+}
+
+// ------------------------------------------------------------ the ghost pass
+// After every stage the ghost cells of the stage output are filled from the
+// inner cells just written (the reference's boundary pass after each step,
+// iosmaug.cpp:1157-1166), and their wave speeds join the stage's maxima (the
+// reference's c_max covers the ghosts).  Each ghost cell gathers its value:
+// from the last direction whose pass writes it, back along the chain of
+// sources (smaug_device.cuh) to an inner cell, negating the fields of the
+// asymm rules on the way; a chain that meets a fixed pass ends at a cell that
+// keeps its loaded value, so the ghost is left alone.
+
+// Ghost cells of a grid: the cells with a coordinate outside [2, n-3].
+template <int D>
+__host__ __device__ inline long long ghost_count(const Geo &g) {
+  long long in = 1;
+  for (int d = 0; d < D; ++d) in *= g.n[d] - 4;
+  return g.N - in;
+}
+
+// Coordinates of ghost k: first the four ghost rows (2-D) or planes (3-D) of
+// the last dim, then, for each inner coordinate of the last dim, the ring of
+// the lower dims.
+template <int D>
+__device__ __forceinline__ void ghost_coords(const Geo &g, long long k, int *c) {
+  const int n0 = g.n[0], n1 = g.n[1];
+  if (D == 2) {
+    if (k < 4LL * n0) {
+      const int r = (int)(k / n0);
+      c[0] = (int)(k - (long long)r * n0);
+      c[1] = r < 2 ? r : n1 - 4 + r;
+    } else {
+      const long long q = k - 4LL * n0;
+      const int r = (int)(q & 3);
+      c[1] = 2 + (int)(q >> 2);
+      c[0] = r < 2 ? r : n0 - 4 + r;
+    }
+    c[2] = 0;
+  } else {
+    const long long pl = (long long)n0 * n1;
+    const int n2 = g.n[2];
+    if (k < 4 * pl) {
+      const int r = (int)(k / pl);
+      const long long q = k - r * pl;
+      c[2] = r < 2 ? r : n2 - 4 + r;
+      c[1] = (int)(q / n0);
+      c[0] = (int)(q - (long long)c[1] * n0);
+    } else {
+      const long long ring = pl - (long long)(n0 - 4) * (n1 - 4);
+      const long long q0 = k - 4 * pl;
+      const long long z = q0 / ring;
+      const long long q = q0 - z * ring;
+      c[2] = 2 + (int)z;
+      if (q < 4LL * n0) {
+        const int r = (int)(q / n0);
+        c[0] = (int)(q - (long long)r * n0);
+        c[1] = r < 2 ? r : n1 - 4 + r;
+      } else {
+        const long long u = q - 4LL * n0;
+        const int r = (int)(u & 3);
+        c[1] = 2 + (int)(u >> 2);
+        c[0] = r < 2 ? r : n0 - 4 + r;
+      }
     }
   }
+}
+
+// Fill ghost k of the stage output and take its wave speeds into red.
+template <int D, typename T>
+__device__ __forceinline__ void ghost_cell(const StageArgs &a, const Geo &g, const Phys &p, long long k, T *red) {
+  using L = Lay<D>;
+  constexpr int NW = L::NW, NB = L::NVAR - NW;
+  constexpr bool MIXED = sizeof(T) == sizeof(float);
+  if (k >= ghost_count<D>(g)) return;
+  int c[3], s[3];
+  ghost_coords<D>(g, k, c);
+  s[0] = c[0];
+  s[1] = c[1];
+  s[2] = c[2];
+  unsigned neg = 0;
+  for (int limit = D - 1; limit >= 0;) {
+    int q = limit, L0 = -1;
+    for (; q >= 0; --q) {
+      bool covers = s[q] < 2 || s[q] > g.n[q] - 3;
+      if (!covers && g.btype[q] == BC_FIXED)
+        for (int e = 0; e < q; ++e)
+          if (s[e] == 0 || s[e] == g.n[e] - 1) covers = true;
+      if (covers) {
+        L0 = q;
+        break;
+      }
+    }
+    if (L0 < 0) break;                      // an inner cell: the source
+    if (g.btype[L0] == BC_FIXED) return;    // keeps its loaded value
+    neg ^= bc_neg(g, L0);
+    s[L0] = bc_source(g.btype[L0], D, g.n[L0], s[L0]);
+    limit = L0 - 1;
+  }
+  const long long j = gidx<D>(g, c), src = gidx<D>(g, s);
+  double ov[NW];
+  if (!MIXED) {
+#pragma unroll
+    for (int f = 0; f < NW; ++f) {
+      double v = a.out[fo32(f, g.N, src)];
+      if ((neg >> f) & 1u) v = -v;
+      a.out[fo32(f, g.N, j)] = v;
+      ov[f] = v;
+    }
+  } else if (a.kind == 4) {
+#pragma unroll
+    for (int f = 0; f < NW; ++f) {
+      float v = a.w32[fo32(f, g.N, src)], w = a.c32[fo32(f, g.N, src)];
+      if ((neg >> f) & 1u) {
+        v = -v;
+        w = -w;
+      }
+      a.w32[fo32(f, g.N, j)] = v;
+      a.c32[fo32(f, g.N, j)] = w;
+      ov[f] = (double)v;
+    }
+  } else {
+#pragma unroll
+    for (int f = 0; f < NW; ++f) {
+      float v = a.out32[fo32(f, g.N, src)];
+      if ((neg >> f) & 1u) v = -v;
+      a.out32[fo32(f, g.N, j)] = v;
+      ov[f] = (double)v;
+    }
+  }
+  double bgv[NB];
+#pragma unroll
+  for (int b = 0; b < NB; ++b)
+    bgv[b] = (b == L::RHOB - NW || p.has_bgb) ? __ldg(a.bg + fo32(b, g.N, j)) : 0.0;
+  if constexpr (MIXED)
+    reduce_cell_mixed<D>(g, p, ov, bgv, j, red);
+  else
+    reduce_cell<D>(g, p, ov, bgv, j, red);
 }
 
 // One RK stage on the tile (bx, by, bz) of one simulation; every thread of
@@ -648,6 +767,17 @@ __global__ void __launch_bounds__(256, 2) tile_stage_kernel(StageArgs a, Geo g, 
   extern __shared__ __align__(16) unsigned char smraw[];
   T red[6] = {0, 0, 0, 0, 0, 0};
   tile_body<D, T, TileShape<D>>(a, g, p, blockIdx.x, blockIdx.y, blockIdx.z, reinterpret_cast<T *>(smraw), red);
+  block_max_flush<6>(red, &a.sc->red[a.red_out]);
+}
+
+// The ghost pass after a tile_stage_kernel launch (grid-stride over the ghosts).
+template <int D, typename T>
+__global__ void __launch_bounds__(256) ghost_stage_kernel(StageArgs a, Geo g, Phys p) {
+  T red[6] = {0, 0, 0, 0, 0, 0};
+  const long long ng = ghost_count<D>(g);
+  const long long step = (long long)gridDim.x * blockDim.x;
+  for (long long k0 = (long long)blockIdx.x * blockDim.x; k0 < ng; k0 += step)
+    ghost_cell<D, T>(a, g, p, k0 + threadIdx.x, red);
   block_max_flush<6>(red, &a.sc->red[a.red_out]);
 }
 

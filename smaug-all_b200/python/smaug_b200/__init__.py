@@ -29,7 +29,8 @@ class Params(ctypes.Structure):
                 ("btype", _I * 3), ("g", _D * 3), ("hyperdif", _I), ("rk4", _I), ("dt_mode", _I),
                 ("dt0", _D), ("exact", _I), ("precision", _I),
                 ("drv_on", _I), ("drv_dir", _I), ("drv_amp", _D), ("drv_period", _D),
-                ("drv_center", _D * 3), ("drv_width", _D * 3), ("xmin", _D * 3), ("dx", _D * 3)]
+                ("drv_center", _D * 3), ("drv_width", _D * 3), ("xmin", _D * 3), ("dx", _D * 3),
+                ("bmask", _I * 3)]
 
 
 PREC_FP64 = 0   # SMAUG_PREC_FP64
@@ -111,6 +112,9 @@ def make_params(prob, rk4: bool = True, dt_mode: int = 1, exact: bool = False, d
         p.n[d] = prob.n[d] if d < prob.ndim else 1
         p.btype[d] = prob.btype[d] if d < prob.ndim else 0
         p.g[d] = prob.g[d] if d < len(prob.g) else 0.0
+    bm = tuple(getattr(prob, "bmask", (0, 0, 0))) + (0, 0, 0)
+    for d in range(3):
+        p.bmask[d] = int(bm[d]) if d < prob.ndim else 0
     p.gamma = prob.gamma
     p.courant = prob.courant
     for f in range(len(prob.chyp)):
