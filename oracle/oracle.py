@@ -42,7 +42,8 @@ class _Driver(ctypes.Structure):
 class _Grid(ctypes.Structure):
     _fields_ = [("ndim", _I), ("n", _I * 3), ("gamma", _D), ("chyp", _D * 13),
                 ("btype", _I * 3), ("g", _D * 3), ("courant", _D), ("hyperdif", _I),
-                ("delx", _PD * 3), ("drv", ctypes.POINTER(_Driver)), ("bmask", _I * 3), ("fixed", _PD)]
+                ("delx", _PD * 3), ("drv", ctypes.POINTER(_Driver)), ("bmask", _I * 3), ("fixed", _PD),
+                ("divb", _I), ("dxs", _D * 3)]
 
 
 class _State(ctypes.Structure):
@@ -103,6 +104,9 @@ class Oracle:
         # before the initial ghost fill, as iosmaug.cpp:645-654 does at it=-1)
         self.fixed = np.ascontiguousarray(prob.w, dtype=np.float64).copy()
         g.fixed = _ptr(self.fixed)
+        g.divb = int(getattr(prob, "divb", 0))
+        for d in range(prob.ndim):
+            g.dxs[d] = float(prob.dx[d])
         self.g = g
         self.s = _State()
         self.s.dt = 1.0e-8 if dt_fixed == 0.0 else dt_fixed
@@ -188,6 +192,8 @@ class Reference:
                 for f in range(nw):
                     if (bm[d] >> f) & 1:
                         L.ref_set_btype(f, d, 7)
+        if getattr(prob, "divb", 0):
+            L.ref_set_divb(1)
         w = np.ascontiguousarray(prob.w)
         L.ref_set_state(_ptr(w))
         self.nstep = 0

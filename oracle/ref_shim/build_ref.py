@@ -61,7 +61,8 @@ ORACLE = HERE.parent
 OUT = ORACLE / "_ref"
 
 # Sources on the single-step hot path (make_inputs:76-98 minus host I/O,
-# the unused hyperdifvisc1.cu, divb.cu (divbon=0) and the MPI layer).
+# the unused hyperdifvisc1.cu and the MPI layer); divb.cu runs when the
+# driver switches divbon / divbfix on.
 KERNEL_SOURCES = {
     # file: [(template source, MODID)] -- Makefile:177-245
     "hyperdifmomsource1.cu": [("gradops.cu", "hdm1")],
@@ -80,6 +81,7 @@ KERNEL_SOURCES = {
     "init.cu": [("gradops.cu", "i"), ("init_user.cu", "i")],
     "update.cu": [("gradops.cu", "u")],
     "advance.cu": [("gradops.cu", "adv"), ("dervfields.cu", "adv")],
+    "divb.cu": [("gradops.cu", "db"), ("dervfields.cu", "db")],
 }
 
 REDUCTIONS = {

@@ -101,6 +101,13 @@ int ref_init(const int *n, const double *xmin, const double *dx, double gamma,
   return 0;
 }
 
+/* divbon and divbfix (the divergence-of-B source terms, divb.cu), after ref_init. */
+int ref_set_divb(int on) {
+  p->divbon = p->divbfix = on;
+  d_p->divbon = d_p->divbfix = on;
+  return 0;
+}
+
 /* Boundary type of one field along one dim (both sides), after ref_init. */
 int ref_set_btype(int field, int dim, int type) {
   if (field < 0 || field >= NVAR || dim < 0 || dim >= NDIM) return -1;
@@ -194,6 +201,7 @@ int ref_step(int n) {
     }
   }
   cugrav(&p, &d_p, &d_state, &d_wmod, &d_wmod, &d_dwn1, &d_wd, order, ordero, p->dt);
+  if (p->divbon == 1) cudivb(&p, &d_p, &d_w, &d_wmod, &d_dwn1, &d_wd, order, ordero, p->dt); /* 962-963 */
 
   if (p->hyperdifmom == 1) { /* 969-1146 */
     dt = (p->dt);

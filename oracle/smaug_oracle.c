@@ -406,6 +406,60 @@ void sm_oracle_boundary(const sm_oracle_grid *g, double *w) {
 
 /* ------------------------------------------------------------- the stage */
 
+/* grad3d_MODID (gradops.cu:132-237, 2-D branch): 4th-order difference over
+ * the uniform spacing p->dx, zero at the first and last two inner cells
+ * whatever the boundary type (the tests read `x==2 || x==3 && ...`, the
+ * second part always true at inner cells). */
+static double grad3d(const sm_oracle_grid *g, const lay_t *L, const double *a, long idx, const int c[3], int dir) {
+  const int n = L->n[dir], x = c[dir], o = 1 - dir;
+  const long s = L->st[dir];
+  double grad = 0;
+  if (x > 1 && x < n - 2)
+    grad = (((8 * a[idx + s] - 8 * a[idx - s] + a[idx - 2 * s] - a[idx + 2 * s]) / 6.0)) / (2.0 * (g->dxs[dir]));
+  const int in_o = c[o] > 1 && c[o] < L->n[o] - 2;
+  if ((x == n - 3) || (x == n - 4 && in_o))
+    grad = 0;
+  else if (x == 2 || (x == 3 && in_o))
+    grad = 0;
+  return grad;
+}
+
+/* divb_parallel (divb.cu:165-336) with divbon = divbfix = 1, 2-D: at cells
+ * 3..n-3 of both dims, divB = d_x b1 + d_y b2 + d_x b1b + d_y b2b and the
+ * sources -divB (0, b, B.v, v) with B.v = (B_total . m) / rho_t
+ * (computebdotv3, dervfields.cu:46-52) and NaN sources taken as 0
+ * (dbsourcemom, dbsourceb); then every inner cell (from 2) takes
+ * w -= dt * source. */
+static void divb_terms(const sm_oracle_grid *g, const lay_t *L, const double *win, double *wout, double h) {
+  const long N = L->N;
+  const int NW = L->NW;
+  double *dw = (double *)calloc((size_t)NW * N, sizeof(double));
+  for (long idx = 0; idx < N; ++idx) {
+    int c[3];
+    coords(L, idx, c);
+    if (!(c[0] > 2 && c[1] > 2 && c[0] < L->n[0] - 2 && c[1] < L->n[1] - 2)) continue;
+    double divb = grad3d(g, L, F(win, L->B0), idx, c, 0) + grad3d(g, L, F(win, L->B0 + 1), idx, c, 1);
+    divb += grad3d(g, L, F(win, L->BB0), idx, c, 0) + grad3d(g, L, F(win, L->BB0 + 1), idx, c, 1);
+    const double rt = F(win, L->RHO)[idx] + F(win, L->RHOB)[idx];
+    const double bdotv = ((F(win, L->B0)[idx] + F(win, L->BB0)[idx]) * F(win, L->M0)[idx] +
+                          (F(win, L->B0 + 1)[idx] + F(win, L->BB0 + 1)[idx]) * F(win, L->M0 + 1)[idx]) / rt;
+    for (int k = 0; k < 2; ++k) {
+      double sm = -divb * F(win, L->B0 + k)[idx];
+      dw[(long)(L->M0 + k) * N + idx] = dw[(long)(L->M0 + k) * N + idx] + (isnan(sm) ? 0 : sm);
+      double sb = -divb * F(win, L->M0 + k)[idx] / (F(win, L->RHO)[idx] + F(win, L->RHOB)[idx]);
+      dw[(long)(L->B0 + k) * N + idx] = dw[(long)(L->B0 + k) * N + idx] + (isnan(sb) ? 0 : sb);
+    }
+    dw[(long)L->EN * N + idx] = dw[(long)L->EN * N + idx] + (-divb * bdotv);
+  }
+  for (long idx = 0; idx < N; ++idx) {
+    int c[3];
+    coords(L, idx, c);
+    if (!(c[0] > 1 && c[1] > 1 && c[0] < L->n[0] - 2 && c[1] < L->n[1] - 2)) continue;
+    for (int f = 0; f < NW; ++f) F(wout, f)[idx] = F(wout, f)[idx] - h * dw[(long)f * N + idx];
+  }
+  free(dw);
+}
+
 /* Driver (usersource.cu.spicule1:4-137) on every cell of wout; the ghost
  * fill that follows overwrites the ghosts, as cuboundary does after cusource
  * (iosmaug.cpp:1153-1166). */
@@ -498,6 +552,9 @@ double sm_oracle_stage_t(const sm_oracle_grid *g, const double *win, const doubl
       F(wout, L->EN)[idx] += (h)*F(win, L->RHO)[idx] * ((g->g[k]) * F(win, L->M0 + k)[idx]) /
                              (F(win, L->RHO)[idx] + F(win, L->RHOB)[idx]);
   }
+
+  /* divergence of B, cudivb (divb.cu:165-336; iosmaug.cpp:962-963): 2-D */
+  if (g->divb && D == 2) divb_terms(g, L, win, wout, h);
 
   if (g->hyperdif) {
     /* ---- density, hyperdifrhosource1.cu:15-282 */

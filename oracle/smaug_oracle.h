@@ -54,6 +54,8 @@ typedef struct {
   const sm_oracle_driver *drv;  /* NULL: no driver */
   int bmask[3];        /* per dim: evolved fields (bit f) that take asymm where btype is symm */
   const double *fixed; /* fixed (5) boundaries: the state as loaded (NVAR * N), or NULL */
+  int divb;            /* 2-D: divergence-of-B source terms (p->divbon, p->divbfix) */
+  double dxs[3];       /* p->dx: the uniform spacing the divB gradient divides by */
 } sm_oracle_grid;
 
 /* Per-run scalars carried between steps (p->dt, p->dtdiffvisc, p->maxviscoef). */

@@ -58,6 +58,8 @@ class Problem:
     driver: dict | None = None
     # per dim: evolved fields (bit f) that take asymm where btype is symm
     bmask: tuple = (0, 0, 0)
+    # 2-D: divergence-of-B source terms (the reference's divbon / divbfix)
+    divb: int = 0
 
     @property
     def ncells(self) -> int:

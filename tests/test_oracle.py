@@ -42,15 +42,20 @@ def test_oracle_reproduces_golden(name):
     assert states_match(o.w, gold["w_final"], spec, meta["source"])
 
 
-def _run_ref_vs_oracle(kind, n, btype, steps, bmask=None):
+def _run_ref_vs_oracle(kind, n, btype, steps, bmask=None, divb=0):
     code = f"""
 import sys, numpy as np
 sys.path.insert(0, {str(ROOT)!r}); sys.path.insert(0, {str(ROOT / 'smaug-all_b200' / 'python')!r})
 from smaug_b200 import problems
 from oracle.oracle import Oracle, Reference
 prob = problems.orszag_tang({n}) if {kind!r} == 'ot' else problems.blast_wave({n}, seed=7)
+if {divb!r}:  # B noise: a divergence for the divB terms to act on
+    rng = np.random.default_rng(5)
+    for k in range(prob.ndim):
+        prob.w[2 + prob.ndim + k] += 0.02 * rng.standard_normal(prob.w.shape[1:])
 if {btype!r}: prob.btype = tuple({btype!r})
 if {bmask!r}: prob.bmask = tuple({bmask!r})
+prob.divb = {divb!r}
 r = Reference(prob); o = Oracle(prob)
 for s in range({steps}):
     wr = r.step(1); wo = o.step(1, rk4=False)
@@ -85,6 +90,24 @@ BOUNDARY_CASES = [
     ("blast", 12, [6, 6, 6], 4, [0b100010, 0b1000100, 0b10001000]), ("blast", 12, [7, 0, 6], 4, None),
     ("blast", 12, [0, 3, 5], 4, None),
 ]
+
+
+@pytest.mark.skipif(not all(p.exists() for p in REF_LIBS), reason="host build of the reference not present")
+@pytest.mark.parametrize("btype", [None, [4, 0], [5, 6]])
+def test_oracle_divb_terms_bit_exact_vs_reference(btype):
+    """Divergence-of-B sources (divb.cu, divbon = divbfix = 1), 2-D."""
+    _run_ref_vs_oracle("ot", 28, btype, 6, None, 1)
+
+
+def test_oracle_divb_terms_act():
+    prob = problems.orszag_tang(24)
+    rng = np.random.default_rng(5)
+    for k in range(2):
+        prob.w[4 + k] += 0.02 * rng.standard_normal(prob.w.shape[1:])
+    a = Oracle(prob).step(3, rk4=True)
+    prob.divb = 1
+    b = Oracle(prob).step(3, rk4=True)
+    assert not np.array_equal(a, b)
 
 
 @pytest.mark.skipif(not all(p.exists() for p in REF_LIBS), reason="host build of the reference not present")
