@@ -126,6 +126,13 @@ typedef struct {
   double dx[3];           /* grid spacing per dim */
   int bmask[3];           /* per dim: evolved fields (bit = field id) that take
                              SMAUG_BC_ASYMM where btype is SMAUG_BC_SYMM */
+  /*
+   * 1: the divergence-of-B source terms of cudivb (divb.cu:165-336, the
+   * reference's divbon = divbfix = 1), after gravity: -divB (0, B, B.v, v)
+   * with divB the 4th-order difference over the spacing dx[] above.  2-D
+   * only (the reference's 3-D kernel reads an uninitialised bound).
+   */
+  int divb;
 } smaug_params;
 
 /* Number of fields for ndim (10 or 13). */

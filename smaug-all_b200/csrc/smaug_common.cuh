@@ -94,6 +94,13 @@ const char *plan_sim(const smaug_params *prm, SimPlan &r) {
   }
   p.hyperdif = prm->hyperdif;
   p.dt_mode = prm->dt_mode;
+  p.divb = prm->divb != 0;
+  for (int d = 0; d < 3; ++d) p.dxs[d] = d < D ? prm->dx[d] : 0.0;
+  if (p.divb) {
+    if (D != 2) return "divb (divergence-of-B terms) is 2-D only";
+    for (int d = 0; d < D; ++d)
+      if (!(prm->dx[d] > 0.0)) return "divb needs the grid spacing dx > 0";
+  }
   p.drv_on = prm->drv_on != 0;
   p.drv_dir = prm->drv_dir;
   p.drv_amp = prm->drv_amp;
@@ -118,15 +125,26 @@ const char *plan_sim(const smaug_params *prm, SimPlan &r) {
 // One direction's pass of the ghost fill of the evolved fields (the rules of
 // smaug_device.cuh, field by field, direction by direction as
 // iosmaug.cpp:1157-1166): the ghost layers of d from their sources along d,
-// which this pass does not write.  Fixed layers, and outermost layers that a
-// later fixed pass restores, keep their values.
+// which this pass does not write.  Fixed layers, and cells that a later fixed
+// pass restores, keep their values.
 __global__ void ghost_pass_kernel(double *w, int nw, Geo g, int D, int d) {
   const int n = g.n[d], t = g.btype[d];
   const unsigned neg = bc_neg(g, d);
   for (long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x; j < g.N; j += (long long)gridDim.x * blockDim.x) {
     const int x = (int)((j / g.st[d]) % n);
     if (x >= 2 && x <= n - 3) continue;
-    if (t == BC_FIXED || (g.outer_frozen[d] && (x == 0 || x == n - 1))) continue;
+    if (t == BC_FIXED) continue;
+    // a later fixed pass restores this cell (its ghost layers, and the
+    // outermost layer of the earlier dims): it keeps its loaded value
+    const int c[3] = {(int)(j % g.n[0]), (int)((j / g.n[0]) % g.n[1]), (int)(j / g.st[2])};
+    bool later_fixed = false;
+    for (int q = d + 1; q < D; ++q) {
+      if (g.btype[q] != BC_FIXED) continue;
+      if (c[q] < 2 || c[q] > g.n[q] - 3) later_fixed = true;
+      for (int e = 0; e < q; ++e)
+        if (c[e] == 0 || c[e] == g.n[e] - 1) later_fixed = true;
+    }
+    if (later_fixed) continue;
     const int xs = bc_source(t, D, n, x);
     const long long src = j + (long long)(xs - x) * g.st[d];
     for (int f = 0; f < nw; ++f) {

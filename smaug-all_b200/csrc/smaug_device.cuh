@@ -69,6 +69,8 @@ struct Phys {
   int has_bgb;                // any background B or eb != 0 (energy background terms)
   int has_grav;
   int dt_mode;
+  int divb;                   // 2-D divergence-of-B source terms (divbon, divbfix)
+  double dxs[3];              // uniform spacing per dim (p->dx, the divB gradient)
   int drv_on, drv_dir;        // momentum driver: on, driven momentum component
   double drv_amp, drv_period; // amplitude, period (0: constant in time)
 };

@@ -29,6 +29,27 @@ __device__ __forceinline__ bool inner_at(const Geo &g, const int *c) {
   return true;
 }
 
+// grad3d_MODID (gradops.cu:132-237, 2-D branch): 4th-order difference of
+// field f along dir over the uniform spacing p->dx, zero at the first and
+// last two inner cells whatever the boundary type (its tests read
+// `x==2 || x==3 && ...`, the second part true at every inner cell).
+template <int D>
+__device__ __forceinline__ double grad3d_at(const Cell<D> &C, const Geo &g, const Phys &p, long long idx, const int *c,
+                                            int f, int dir) {
+  const int n = g.n[dir], x = c[dir], o = 1 - dir;
+  const long long s = g.st[dir];
+  double grad = 0;
+  if (x > 1 && x < n - 2)
+    grad = (((8 * C.v(f, idx + s) - 8 * C.v(f, idx - s) + C.v(f, idx - 2 * s) - C.v(f, idx + 2 * s)) / 6.0)) /
+           (2.0 * (p.dxs[dir]));
+  const bool in_o = c[o] > 1 && c[o] < g.n[o] - 2;
+  if ((x == n - 3) || (x == n - 4 && in_o))
+    grad = 0;
+  else if (x == 2 || (x == 3 && in_o))
+    grad = 0;
+  return grad;
+}
+
 // Block-wide max of v[0..5] then one atomic per value into r.
 template <int NV>
 __device__ __forceinline__ void block_max_flush(double *v, Reduce *r) {
@@ -231,6 +252,24 @@ __global__ void __launch_bounds__(kBX *kBY) stage_kernel(StageArgs a, Geo g, Phy
 #pragma unroll
       for (int k = 0; k < D; ++k)
         o[L::EN] += (h)*C.v(L::RHO, idx) * ((p.g[k]) * C.v(L::M0 + k, idx)) / (C.v(L::RHO, idx) + C.v(L::RHOB, idx));
+    }
+
+    // ---- divergence of B (cudivb, divb.cu:165-336; iosmaug.cpp:962-963), 2-D:
+    // divB at cells 3..n-3, sources -divB (0, B, B.v, v), w -= dt * source
+    if (D == 2 && p.divb && c[0] > 2 && c[1] > 2) {
+      double divb = grad3d_at<D>(C, g, p, idx, c, L::B0, 0) + grad3d_at<D>(C, g, p, idx, c, L::B0 + 1, 1);
+      divb += grad3d_at<D>(C, g, p, idx, c, L::BB0, 0) + grad3d_at<D>(C, g, p, idx, c, L::BB0 + 1, 1);
+      const double bdotv = ((C.v(L::B0, idx) + C.v(L::BB0, idx)) * C.v(L::M0, idx) +
+                            (C.v(L::B0 + 1, idx) + C.v(L::BB0 + 1, idx)) * C.v(L::M0 + 1, idx)) /
+                           (C.v(L::RHO, idx) + C.v(L::RHOB, idx));
+#pragma unroll
+      for (int k = 0; k < 2; ++k) {
+        const double sm = -divb * C.v(L::B0 + k, idx);
+        o[L::M0 + k] = o[L::M0 + k] - h * (0.0 + (isnan(sm) ? 0 : sm));
+        const double sb = -divb * C.v(L::M0 + k, idx) / (C.v(L::RHO, idx) + C.v(L::RHOB, idx));
+        o[L::B0 + k] = o[L::B0 + k] - h * (0.0 + (isnan(sb) ? 0 : sb));
+      }
+      o[L::EN] = o[L::EN] - h * (0.0 + (-divb * bdotv));
     }
 
     if (p.hyperdif) {

@@ -321,6 +321,46 @@ __device__ __forceinline__ void stage_epilogue(const StageArgs &a, const Geo &g,
   }
 }
 
+// Divergence-of-B source terms at an inner cell (cudivb, divb.cu:165-336 with
+// divbon = divbfix = 1; 2-D): at cells 3..n-3 of both dims, divB from the
+// 4th-order difference over the uniform spacing (zero at the first and last
+// two inner cells, as grad3d of gradops.cu:132-237), then -divB (0, B, B.v,
+// v) per unit time with B.v = B_total . m / rho_t; NaN momentum and field
+// sources count as 0 (dbsourcemom, dbsourceb).
+template <typename T>
+__device__ __forceinline__ void divb_sources(const CellT<2, T> &C, const Geo &g, const Phys &p, const int *c,
+                                             long long idx, T *dL) {
+  using L = Lay<2>;
+  if (c[0] <= 2 || c[1] <= 2) return;
+  T divb = 0;
+#pragma unroll
+  for (int d = 0; d < 2; ++d) {
+    const int x = c[d], n = g.n[d];
+    if (x == 3 || x == n - 4 || x == n - 3) continue;
+    const long long s = g.st[d];
+    T b[4];  // B_d + B_bd at -2, -1, +1, +2
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const long long j = idx + (k < 2 ? k - 2 : k - 1) * s;
+      b[k] = C.v(L::B0 + d, j) + (p.has_bgb ? C.v(L::BB0 + d, j) : T(0));
+    }
+    divb += ((T)8 * (b[2] - b[1]) - (b[3] - b[0])) * (T)(1.0 / (12.0 * p.dxs[d]));
+  }
+  const T irt = (T)(1.0 / (C.vd(L::RHO, idx) + C.vd(L::RHOB, idx)));
+  T bdotv = 0;
+#pragma unroll
+  for (int k = 0; k < 2; ++k) {
+    const T bk = C.v(L::B0 + k, idx), mk = C.v(L::M0 + k, idx);
+    bdotv += (bk + (p.has_bgb ? C.v(L::BB0 + k, idx) : T(0))) * mk;
+    T sm = divb * bk, sb = divb * mk * irt;
+    if (sm != sm) sm = 0;
+    if (sb != sb) sb = 0;
+    dL[L::M0 + k] += sm;
+    dL[L::B0 + k] += sb;
+  }
+  dL[L::EN] += divb * bdotv * irt;
+}
+
 // ------------------------------------------------------------ the ghost pass
 // After every stage the ghost cells of the stage output are filled from the
 // inner cells just written (the reference's boundary pass after each step,
@@ -544,6 +584,9 @@ __device__ __forceinline__ void tile_body(const StageArgs &a, const Geo &g, cons
       dL[L::M0 + k] += (T)p.g[k] * rho;
       dL[L::EN] += rho * (T)p.g[k] * C.v(L::M0 + k, idx) * irt;
     }
+  }
+  if constexpr (D == 2) {
+    if (active && p.divb) divb_sources<T>(C, g, p, c, idx, dL);
   }
 
   // ------------------------------------------------ per-dimension hyperdiffusion

@@ -231,6 +231,7 @@ __device__ __forceinline__ void tile_body2(const StageArgs &a, const Geo &g, con
         dL[L::EN] += rho * (T)p.g[k] * C.v(L::M0 + k, idx) * irt;
       }
     }
+    if (p.divb) divb_sources<T>(C, g, p, c, idx, dL);
     const int r0 = (tx + 3) + B::QX * (ty + 3);
     // the terms along dimension d (a compile-time constant in each call, so
     // that nothing indexes Geo, c, cm or idx1 dynamically)

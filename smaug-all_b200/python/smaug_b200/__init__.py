@@ -30,7 +30,7 @@ class Params(ctypes.Structure):
                 ("dt0", _D), ("exact", _I), ("precision", _I),
                 ("drv_on", _I), ("drv_dir", _I), ("drv_amp", _D), ("drv_period", _D),
                 ("drv_center", _D * 3), ("drv_width", _D * 3), ("xmin", _D * 3), ("dx", _D * 3),
-                ("bmask", _I * 3)]
+                ("bmask", _I * 3), ("divb", _I)]
 
 
 PREC_FP64 = 0   # SMAUG_PREC_FP64
@@ -116,6 +116,7 @@ def make_params(prob, rk4: bool = True, dt_mode: int = 1, exact: bool = False, d
     for d in range(3):
         p.bmask[d] = int(bm[d]) if d < prob.ndim else 0
     p.gamma = prob.gamma
+    p.divb = int(getattr(prob, "divb", 0))
     p.courant = prob.courant
     for f in range(len(prob.chyp)):
         p.chyp[f] = float(prob.chyp[f])

@@ -35,14 +35,29 @@ CASES = [
     ("blast", 14, (5, 5, 5), None, True, 4),
     ("blast", 14, (6, 6, 6), (0b100010, 0b1000100, 0b10001000), True, 4),
     ("blast", 14, (0, 3, 5), None, False, 4),
+    ("ot", 36, (4, 5), None, True, 5),
+    ("blast", 14, (4, 6, 5), None, True, 4),
 ]
 
 
 def make(kind, n, btype, bmask):
+    """The state's ghost cells get noise, so that they match no fill rule:
+    fixed ghosts, and the cells the fill takes from them, then differ from
+    anything a wrong fill would write."""
     prob = problems.orszag_tang(n) if kind == "ot" else problems.blast_wave(n, seed=11)
     prob.btype = tuple(btype)
     if bmask:
         prob.bmask = tuple(bmask)
+    D = prob.ndim
+    ghost = np.zeros(prob.w.shape[1:], dtype=bool)
+    for d in range(D):
+        sl = [slice(None)] * D
+        ax = D - 1 - d
+        sl[ax] = np.r_[0, 1, prob.n[d] - 2, prob.n[d] - 1]
+        ghost[tuple(sl)] = True
+    rng = np.random.default_rng(21)
+    for f in range(2 + 2 * D):
+        prob.w[f][ghost] *= 1.0 + 0.01 * rng.standard_normal(int(ghost.sum()))
     return prob
 
 

@@ -42,7 +42,7 @@ def test_oracle_reproduces_golden(name):
     assert states_match(o.w, gold["w_final"], spec, meta["source"])
 
 
-def _run_ref_vs_oracle(kind, n, btype, steps, bmask=None, divb=0):
+def _run_ref_vs_oracle(kind, n, btype, steps, bmask=None, divb=0, noise_ghosts=False):
     code = f"""
 import sys, numpy as np
 sys.path.insert(0, {str(ROOT)!r}); sys.path.insert(0, {str(ROOT / 'smaug-all_b200' / 'python')!r})
@@ -56,6 +56,13 @@ if {divb!r}:  # B noise: a divergence for the divB terms to act on
 if {btype!r}: prob.btype = tuple({btype!r})
 if {bmask!r}: prob.bmask = tuple({bmask!r})
 prob.divb = {divb!r}
+if {btype!r} and {noise_ghosts!r}:  # ghosts that match no fill rule
+    D = prob.ndim; gh = np.zeros(prob.w.shape[1:], dtype=bool)
+    for d in range(D):
+        sl = [slice(None)] * D; sl[D - 1 - d] = np.r_[0, 1, prob.n[d] - 2, prob.n[d] - 1]; gh[tuple(sl)] = True
+    rng = np.random.default_rng(21)
+    for f in range(2 + 2 * D):
+        prob.w[f][gh] *= 1.0 + 0.01 * rng.standard_normal(int(gh.sum()))
 r = Reference(prob); o = Oracle(prob)
 for s in range({steps}):
     wr = r.step(1); wo = o.step(1, rk4=False)
@@ -89,6 +96,7 @@ BOUNDARY_CASES = [
     ("blast", 12, [3, 3, 0], 4, None), ("blast", 12, [5, 5, 5], 4, None),
     ("blast", 12, [6, 6, 6], 4, [0b100010, 0b1000100, 0b10001000]), ("blast", 12, [7, 0, 6], 4, None),
     ("blast", 12, [0, 3, 5], 4, None),
+    ("ot", 24, [4, 5], 5, None), ("blast", 12, [4, 6, 5], 4, None),
 ]
 
 
@@ -113,7 +121,7 @@ def test_oracle_divb_terms_act():
 @pytest.mark.skipif(not all(p.exists() for p in REF_LIBS), reason="host build of the reference not present")
 @pytest.mark.parametrize("kind,n,btype,steps,bmask", BOUNDARY_CASES)
 def test_oracle_boundary_types_bit_exact_vs_reference(kind, n, btype, steps, bmask):
-    _run_ref_vs_oracle(kind, n, btype, steps, bmask)
+    _run_ref_vs_oracle(kind, n, btype, steps, bmask, noise_ghosts=True)
 
 
 def test_metric_is_tensor_product_inside():
