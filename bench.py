@@ -438,6 +438,66 @@ def run_blast(a, ctx):
     return out
 
 
+def run_atmos3d(a, ctx):
+    """Stratified solar atmosphere, 3-D: 256 (z, vertical) x 128 x 128 cells over
+    6 x 4 x 4 Mm; hydrostatic split background (T(z) tanh profile, rho_b by
+    FP64 trapezoid from 2.7e-4 kg/m^3, uniform vertical B_b = 10 G); lower
+    boundary vertical-velocity driver (300 s, 200 m/s, 0.5 Mm); vertical
+    contcd4, lateral periodic; gravity.  Single simulation, mixed and FP64,
+    then the mixed state's relative L2 difference from the FP64 one after the
+    same steps."""
+    import numpy as np
+
+    from smaug_b200 import PREC_FP64, PREC_MIXED, Engine, problems
+    prob = problems.atmosphere(256, 128, 128)
+    n_int = prob.interior
+    peak, _ = load_peaks()
+    out = {"workload": "stratified atmosphere 3-D, 256 (z) x 128 x 128 cells over 6 x 4 x 4 Mm, hydrostatic "
+                       "background, 10 G vertical B_b, lower-boundary driver 300 s / 200 m/s / 0.5 Mm, vertical "
+                       "contcd4, lateral periodic, gravity, RK4, single simulation",
+           "interior_cells": n_int}
+    states = {}
+    for name, prec, bpc in (("mixed", PREC_MIXED, BYTES_PER_CELL_UPDATE_MIXED_3D),
+                            ("fp64", PREC_FP64, BYTES_PER_CELL_UPDATE_FP64_3D)):
+        eng = Engine(prob, rk4=True, device=ctx.local, precision=prec)
+        m = measure(eng, n_int, a.steps, a.warmup, ctx, sample_clocks=False)
+        alg = bpc / 4 * n_int
+        ach = alg / (m["avg_stage_ms"] / 1e3) / 1e9
+        out[name] = {"value": m["value"], "ms_per_step": m["ms_per_step"], "avg_stage_ms": m["avg_stage_ms"],
+                     "roofline": {"achieved": ach, "peak": peak, "frac": ach / peak, "unit": "GB/s",
+                                  "alg_bytes_per_launch": alg}}
+        states[name] = (eng.state(), eng.scalars()["steps"])
+        eng.close()
+    out["mixed_vs_fp64"] = out["mixed"]["value"] / out["fp64"]["value"]
+    wm, sm = states["mixed"]
+    wf, sf = states["fp64"]
+    nw = 2 + 2 * prob.ndim
+    sl = (slice(None),) + tuple(slice(2, -2) for _ in range(prob.ndim))
+    rel = []
+    for f in range(nw):
+        nb = float(np.linalg.norm(wf[sl][f]))
+        rel.append(float(np.linalg.norm(wm[sl][f] - wf[sl][f]) / nb) if nb > 0 else None)
+    out["mixed_vs_fp64_rel_l2_per_field"] = {"steps": sm, "same_steps": sm == sf, "fields": rel,
+                                              "dt": "each path's own dt rule"}
+    # the same comparison at one fixed dt: the dt rule's viscous limit comes
+    # from hyperviscosity that the method computes from rounding noise in the
+    # flat corona, so paths that round differently pick slightly different dt
+    # and then drift apart; at a fixed dt what remains is the arithmetic
+    dt0 = 0.1
+    fixed = {}
+    for name, prec in (("mixed", PREC_MIXED), ("fp64", PREC_FP64)):
+        eng = Engine(prob, rk4=True, device=ctx.local, precision=prec, dt_mode=0, dt0=dt0)
+        eng.step(20)
+        fixed[name] = eng.state()
+        eng.close()
+    rel = []
+    for f in range(nw):
+        nb = float(np.linalg.norm(fixed["fp64"][sl][f]))
+        rel.append(float(np.linalg.norm(fixed["mixed"][sl][f] - fixed["fp64"][sl][f]) / nb) if nb > 0 else None)
+    out["mixed_vs_fp64_rel_l2_fixed_dt"] = {"steps": 20, "dt": dt0, "fields": rel}
+    return out
+
+
 def run_serving(a, ctx):
     """Serving stream: Poisson arrivals (40/s, seed 777) of driven
     stratified-atmosphere x-z slices, sizes {128x256 .. 512x1024}, driver
@@ -471,6 +531,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain", action="store_true", help="skip the plain FP64 single-simulation ensemble run")
     ap.add_argument("--no-blast", action="store_true", help="skip the 3-D blast wave measurements")
+    ap.add_argument("--no-atmos3d", action="store_true", help="skip the 3-D stratified atmosphere measurements")
     ap.add_argument("--only-batched", action="store_true", help="just the timed batched run (profiling)")
     ap.add_argument("--ensemble-count", type=int, default=ENSEMBLE["count"])
     ap.add_argument("--serve-requests", type=int, default=48,
@@ -500,6 +561,8 @@ def main():
         e2e = run_e2e_batched(probs, PREC_MIXED, ctx, K)
         if not a.no_blast:
             line_extra["blast128"] = run_blast(a, ctx)
+        if not a.no_atmos3d:
+            line_extra["atmos3d"] = run_atmos3d(a, ctx)
         if a.serve_requests > 0:
             line_extra["serving"] = run_serving(a, ctx)
     else:
