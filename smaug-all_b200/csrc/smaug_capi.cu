@@ -48,7 +48,22 @@ struct Run : SimPlan {
   // optional per-stage timing
   std::vector<cudaEvent_t> *ev = nullptr;
   size_t *ev_used = nullptr;
+  // production RK4 path: CUDA graphs of kGraphSteps steps and of one step
+  // (their kernel arguments hold the buffers and the physics; dropped when
+  // those change)
+  cudaGraphExec_t graph[2] = {nullptr, nullptr};
+  long long graph_launches = 0;  // kernel launches per step in the graphs
 };
+
+constexpr int kGraphSteps = 16;
+
+void drop_graphs(Run &r) {
+  for (auto &g : r.graph)
+    if (g) {
+      cudaGraphExecDestroy(g);
+      g = nullptr;
+    }
+}
 
 __global__ void dt_kernel(DevScalars *sc, Phys p, int D) {
   if (threadIdx.x == 0 && blockIdx.x == 0) {
@@ -361,6 +376,7 @@ int smaug_destroy(smaug_ctx *ctx) {
   cudaFree(ctx->dxlast);
   cudaFree(r.sc);
   cudaFree(r.inst);
+  drop_graphs(r);
   for (auto e : ctx->ev) cudaEventDestroy(e);
   if (r.stream) cudaStreamDestroy(r.stream);
   delete ctx;
@@ -403,6 +419,7 @@ static int load_state(smaug_ctx *ctx, const double *w, size_t count, cudaMemcpyK
   const long long N = r.geo.N;
   if (count != (size_t)r.NVAR * (size_t)N) return fail(ctx, SMAUG_ERR_ARG, "state must hold NVAR * N doubles");
   CK(cudaSetDevice(ctx->device));
+  const Phys before = r.phys;
   CK(cudaMemcpyAsync(r.W[0], w, sizeof(double) * N * r.NW, kind, r.stream));
   CK(cudaMemcpyAsync(r.bg, w + (size_t)N * r.NW, sizeof(double) * N * r.NB, kind, r.stream));
   // host-side scan of the backgrounds: are the energy background terms live?
@@ -422,6 +439,8 @@ static int load_state(smaug_ctx *ctx, const double *w, size_t count, cudaMemcpyK
   CK(run_upload_inst(r));
   CK(cudaStreamSynchronize(r.stream));
   ctx->have_state = true;
+  // the graphs hold the physics by value (dt kernel): recapture if it changed
+  if (memcmp(&before, &r.phys, sizeof(Phys)) != 0) drop_graphs(r);
   ctx->steps = 0;
   return SMAUG_OK;
 }
@@ -454,13 +473,50 @@ int smaug_get_state_device(smaug_ctx *ctx, double *w, size_t count) {
   return store_state(ctx, w, count, cudaMemcpyDeviceToDevice, false);
 }
 
+// The steps of the production RK4 path as graph replays: the launch sequence
+// of a step is the same every step (the batch stage kernel over this
+// simulation's one-entry table, its ghost pass, the dt and finish kernels).
+cudaError_t run_steps_graphed(Run &r, int nsteps) {
+  const int len[2] = {kGraphSteps, 1};
+  for (int k = 0; k < 2; ++k) {
+    if (r.graph[k]) continue;
+    cudaGraph_t g = nullptr;
+    cudaError_t e = cudaStreamBeginCapture(r.stream, cudaStreamCaptureModeThreadLocal);
+    if (e != cudaSuccess) return e;
+    const long long l0 = r.launches;
+    e = run_steps(r, len[k]);
+    const cudaError_t e2 = cudaStreamEndCapture(r.stream, &g);
+    r.graph_launches = (r.launches - l0) / len[k];
+    r.launches = l0;
+    if (e != cudaSuccess) return e;
+    if (e2 != cudaSuccess) return e2;
+    e = cudaGraphInstantiate(&r.graph[k], g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) return e;
+  }
+  for (; nsteps >= kGraphSteps; nsteps -= kGraphSteps) {
+    const cudaError_t e = cudaGraphLaunch(r.graph[0], r.stream);
+    if (e != cudaSuccess) return e;
+    r.launches += r.graph_launches * kGraphSteps;
+  }
+  for (; nsteps > 0; --nsteps) {
+    const cudaError_t e = cudaGraphLaunch(r.graph[1], r.stream);
+    if (e != cudaSuccess) return e;
+    r.launches += r.graph_launches;
+  }
+  return cudaSuccess;
+}
+
 int smaug_step(smaug_ctx *ctx, int nsteps) {
   if (!ctx || nsteps < 0) return SMAUG_ERR_ARG;
   if (!ctx->have_state) return fail(ctx, SMAUG_ERR_STATE, "no state loaded");
   CK(cudaSetDevice(ctx->device));
   Run &r = ctx->run;
   r.ev_used = ctx->profile ? &ctx->ev_used : nullptr;
-  CK(run_steps(r, nsteps));
+  if (r.rk4 && !r.exact && !ctx->profile)
+    CK(run_steps_graphed(r, nsteps));
+  else
+    CK(run_steps(r, nsteps));
   ctx->steps += nsteps;
   return SMAUG_OK;
 }
