@@ -184,10 +184,12 @@ int rebuild(smaug_batch *b) {
   for (int i = 0; i < b->max_inst; ++i) {
     if (!b->slots[i].used) continue;
     set_tiles(b, b->h_tab[i]);
-    const int nt = b->h_tab[i].tiles[0] * b->h_tab[i].tiles[1] * b->h_tab[i].tiles[2];
-    for (int t = 0; t < nt; ++t) w.push_back({i, t});
+    const int *tl = b->h_tab[i].tiles;
+    for (int z = 0; z < tl[2]; ++z)
+      for (int y = 0; y < tl[1]; ++y)
+        for (int x = 0; x < tl[0]; ++x) w.push_back({i, x, y, z});
     const long long ng = ghost_cells(b->h_tab[i].geo, b->D);
-    for (long long t = 0; t < (ng + 255) / 256; ++t) gw.push_back({i, (int)t});
+    for (long long t = 0; t < (ng + 255) / 256; ++t) gw.push_back({i, (int)t, 0, 0});
   }
   if (gw.size() > b->gwork_cap) {
     BK(cudaStreamSynchronize(b->stream));

@@ -21,7 +21,8 @@ struct BatchInst {
 // Work list entry: simulation slot and tile index within it.
 struct WorkItem {
   int inst;
-  int tile;
+  int tile;    // stage items: the tile's x index; ghost items: the chunk
+  int by, bz;  // stage items: the tile's y and z indices
 };
 
 // Tile shapes and occupancy targets (resident blocks per SM the register
@@ -64,7 +65,7 @@ __host__ __device__ inline BatchVariant batch_variant(int D, int v) {
 // and a single-simulation context on the same variant give the same bits.
 __host__ __device__ inline int batch_default_variant(int D, bool mixed) {
   if (D == 2) return mixed ? 8 : 0;
-  return mixed ? 3 : 0;
+  return mixed ? 5 : 0;
 }
 
 __host__ __device__ inline void batch_tile_shape(int D, int v, int *t) {

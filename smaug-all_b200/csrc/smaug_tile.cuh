@@ -22,6 +22,7 @@
 // itself and the dt reductions.  With T = double every expression below is
 // the FP64 path's.
 #pragma once
+#include <type_traits>
 #include "smaug_device.cuh"
 
 namespace SMAUG_NS {
@@ -590,9 +591,9 @@ __device__ __forceinline__ void tile_body(const StageArgs &a, const Geo &g, cons
   }
 
   // ------------------------------------------------ per-dimension hyperdiffusion
-#pragma unroll
-  for (int d = 0; d < D; ++d) {
-    if (!p.hyperdif && !p.has_bgb) break;
+  // (one call per dimension, d a compile-time constant in each)
+  auto dim_pass = [&](auto dc) {
+    constexpr int d = decltype(dc)::value;
     // q box: tile widened by 3 along d and 1 across
     TileBox<D> qb;
 #pragma unroll
@@ -602,17 +603,20 @@ __device__ __forceinline__ void tile_body(const StageArgs &a, const Geo &g, cons
       qb.ext[e] = tile_ext[e] + 2 * w;
     }
     const int nq = qb.size();
-    // nu box: the tile widened by 1 across d (off-diagonal terms need nu there)
-    TileBox<D> nb;
+    // face box: the faces along d of the tile (face j between cells j and
+    // j+1, j from -1), widened by 1 across d (the off-diagonal terms need nu
+    // there); it holds the hyperviscosity ratio max|d3 q| / max|d1 q| per face
+    constexpr int TD = d == 0 ? TX : d == 1 ? TY : TZ;
+    TileBox<D> fb;
 #pragma unroll
     for (int e = 0; e < 3; ++e) {
       const int w = (e >= D || e == d) ? 0 : 1;
-      nb.lo[e] = org[e] - w;
-      nb.ext[e] = tile_ext[e] + 2 * w;
+      fb.lo[e] = org[e] - (e == d ? 1 : w);
+      fb.ext[e] = e == d ? TD + 1 : tile_ext[e] + 2 * w;
     }
-    const int nn = nb.size();
-    T *Q = sm;             // [NQ][nq]
-    T *NU = sm + NQ * nq;  // [2*NQ][nn]: nu_R, nu_L per q slot
+    const int nf = fb.size();
+    T *Q = sm;            // [NQ][nq]
+    T *V = sm + NQ * nq;  // [NQ][nf]
     for (int r = t; r < nq; r += NT) {
       int cc[3];
       qb.at(r, cc);
@@ -636,53 +640,50 @@ __device__ __forceinline__ void tile_body(const StageArgs &a, const Geo &g, cons
     __syncthreads();
     const int sd = d == 0 ? 1 : d == 1 ? qb.ext[0] : qb.ext[0] * qb.ext[1];
     if (p.hyperdif) {
-      for (int r = t; r < nn; r += NT) {
-        int cc[3];
-        nb.at(r, cc);
-        bool inner = true;
+      // runs of SEG faces along d of one q slot on one line: the line's q
+      // values are read once, each first and third difference is formed once
+      // (explicit FMA), every face takes its windowed maxima; the last run of
+      // a line is shifted back to end at the line's last face (shared faces
+      // are written twice with the same value)
+      constexpr int SEG = TD + 1 < 5 ? TD + 1 : 5;
+      constexpr int NS = (TD + 1 + SEG - 1) / SEG;
+      const int lines = nf / (TD + 1);
+      const int fs = d == 0 ? 1 : d == 1 ? fb.ext[0] : fb.ext[0] * fb.ext[1];  // face stride along d
+      for (int u = t; u < NQ * lines * NS; u += NT) {
+        const int sg = u % NS, rest = u / NS;
+        const int ln = rest % lines, k = rest / lines;
+        const int f0 = min(-1 + sg * SEG, TD - SEG);  // first face of the run, tile-relative
+        // the line's cross coordinates (tile-relative, -1 .. T_e): decode ln
+        int cr[3] = {0, 0, 0}, rem = ln;
 #pragma unroll
-        for (int e = 0; e < D; ++e)
-          if (cc[e] < 2 || cc[e] > g.n[e] - 3) inner = false;
-        T nr[NQ], nl[NQ];
-#pragma unroll
-        for (int k = 0; k < NQ; ++k) {
-          nr[k] = 0;
-          nl[k] = 0;
+        for (int e = 0; e < 3; ++e) {
+          if (e == d || e >= D) continue;
+          const int ex = tile_ext[e] + 2;
+          cr[e] = rem % ex - 1;
+          rem /= ex;
         }
-        if (inner) {
-          const int rq = qb.index(cc);
-          const T dxd = (T)__ldg(g.dx1[d] + cc[d]);
+        // q at the cells f0-2 .. f0+SEG+2 along d
+        int qc[3] = {org[0] + cr[0], org[1] + cr[1], org[2] + cr[2]};
+        qc[d] = org[d] + f0 - 2;
+        const T *qq = Q + k * nq + qb.index(qc);
+        T qv[SEG + 5], t1[SEG + 4], t3[SEG + 3];
 #pragma unroll
-          for (int k = 0; k < NQ; ++k) {
-            const T *qq = Q + k * nq + rq;
-            T qv[7];
+        for (int jx = 0; jx < SEG + 5; ++jx) qv[jx] = qq[jx * sd];
 #pragma unroll
-            for (int o = -3; o <= 3; ++o) qv[o + 3] = qq[o * sd];
-            T m3r = 0, m1r = 0, m3l = 0, m1l = 0;
+        for (int jx = 0; jx < SEG + 4; ++jx) t1[jx] = qv[jx + 1] - qv[jx];
 #pragma unroll
-            for (int s2 = -1; s2 <= 1; ++s2) {
-              m3r = vmax(m3r, vabs((T)3 * (qv[s2 + 4] - qv[s2 + 3]) - (qv[s2 + 5] - qv[s2 + 2])));
-              m3l = vmax(m3l, vabs((T)3 * (qv[s2 + 3] - qv[s2 + 2]) - (qv[s2 + 4] - qv[s2 + 1])));
-            }
+        for (int jx = 1; jx <= SEG + 2; ++jx) t3[jx] = vabs(vfma((T)3, t1[jx], -(qv[jx + 2] - qv[jx - 1])));
+        int fc[3] = {org[0] + cr[0], org[1] + cr[1], org[2] + cr[2]};
+        fc[d] = org[d] + f0;
+        T *dst = V + k * nf + fb.index(fc);
 #pragma unroll
-            for (int s2 = -2; s2 <= 2; ++s2) {
-              m1r = vmax(m1r, vabs(qv[s2 + 4] - qv[s2 + 3]));
-              m1l = vmax(m1l, vabs(qv[s2 + 3] - qv[s2 + 2]));
-            }
-            int fid = k == 0 ? L::RHO : k == 1 ? L::EN : k < 2 + D ? L::M0 + (k - 2) : 0;
-            if (k >= 2 + D) {
-              const int ff = k - (2 + D);
-              fid = L::B0 + (ff >= d ? ff + 1 : ff);
-            }
-            const T kk = dxd * cm[d] * (T)p.chyp[fid];
-            nr[k] = m1r > 0 ? kk * m3r / m1r : T(0);
-            nl[k] = m1l > 0 ? kk * m3l / m1l : T(0);
-          }
-        }
+        for (int m = 0; m < SEG; ++m) {
+          T m1 = 0, m3 = 0;
 #pragma unroll
-        for (int k = 0; k < NQ; ++k) {
-          NU[(2 * k) * nn + r] = nr[k];
-          NU[(2 * k + 1) * nn + r] = nl[k];
+          for (int jx = m; jx <= m + 4; ++jx) m1 = vmax(m1, vabs(t1[jx]));
+#pragma unroll
+          for (int jx = m + 1; jx <= m + 3; ++jx) m3 = vmax(m3, t3[jx]);
+          dst[m * fs] = m1 > 0 ? vratio(m3, m1) : T(0);
         }
       }
     }
@@ -690,7 +691,22 @@ __device__ __forceinline__ void tile_body(const StageArgs &a, const Geo &g, cons
     if (active) {
       int cc[3] = {c[0], c[1], c[2]};
       const int r0 = qb.index(cc);
-      const int n0 = nb.index(cc);
+      const int fr = fb.index(cc);  // the cell's right face along d; its left face is fr - fs
+      const int fs = d == 0 ? 1 : d == 1 ? fb.ext[0] : fb.ext[0] * fb.ext[1];
+      const T dxd = (T)__ldg(g.dx1[d] + c[d]);
+      // nu_R, nu_L of slot k at the cell shifted by `off` faces across d: dx
+      // c_max c_hyp times the face ratios (0 off the inner cells, as the
+      // reference's viscosity arrays are)
+      auto nu_at = [&](int k, int off, bool in, T &nr, T &nl) {
+        int fid = k == 0 ? L::RHO : k == 1 ? L::EN : k < 2 + D ? L::M0 + (k - 2) : 0;
+        if (k >= 2 + D) {
+          const int ff = k - (2 + D);
+          fid = L::B0 + (ff >= d ? ff + 1 : ff);
+        }
+        const T kk = dxd * cm[d] * (T)p.chyp[fid];
+        nr = in ? kk * V[k * nf + fr + off] : T(0);
+        nl = in ? kk * V[k * nf + fr - fs + off] : T(0);
+      };
       const long long sg = g.st[d];
       const bool zd = z1(g, c, d);
       const T i1 = idx1[d], i2 = idx1[d] * idx1[d];
@@ -710,12 +726,17 @@ __device__ __forceinline__ void tile_body(const StageArgs &a, const Geo &g, cons
       }
       if (p.hyperdif) {
 #pragma unroll
-        for (int k = 0; k < NQ; ++k) numax = vmax(numax, vmax(NU[2 * k * nn + n0], NU[(2 * k + 1) * nn + n0]));
+        for (int k = 0; k < NQ; ++k) {
+          T nr, nl;
+          nu_at(k, 0, true, nr, nl);
+          numax = vmax(numax, vmax(nr, nl));
+        }
         // rho and internal energy: f += (nu_R dq+ - nu_L dq-) / dx^2
 #pragma unroll
         for (int k = 0; k < 2; ++k) {
           const T *q = Q + k * nq + r0;
-          const T nr = NU[2 * k * nn + n0], nl = NU[(2 * k + 1) * nn + n0];
+          T nr, nl;
+          nu_at(k, 0, true, nr, nl);
           const T dp = zd ? T(0) : q[sd] - q[0], dm = zd ? T(0) : q[0] - q[-sd];
           dL[k == 0 ? L::RHO : L::EN] += (nr * dp - nl * dm) * i2;
         }
@@ -727,7 +748,8 @@ __device__ __forceinline__ void tile_body(const StageArgs &a, const Geo &g, cons
         for (int f = 0; f < D; ++f) {
           const int k = 2 + f;
           const T *v = Q + k * nq + r0;
-          const T nr = NU[2 * k * nn + n0], nl = NU[(2 * k + 1) * nn + n0];
+          T nr, nl;
+          nu_at(k, 0, true, nr, nl);
           const T dvp = zd ? T(0) : v[sd] - v[0], dvm = zd ? T(0) : v[0] - v[-sd];
           const T m0 = C.v(L::M0 + f, idx), mp = C.v(L::M0 + f, idx + sg), mm = C.v(L::M0 + f, idx - sg);
           const T fac = (f == d ? (T)1 : (T)0.5) * i2;
@@ -735,17 +757,19 @@ __device__ __forceinline__ void tile_body(const StageArgs &a, const Geo &g, cons
           dL[L::EN] += ((m0 + mp) * nr * dvp - (m0 + mm) * nl * dvm) * (T)0.5 * fac;
           if (f != d) {  // off-diagonal: m_d += d_f( rho_t (nu_R+nu_L)/4 d_d v_f )
             const int sf = f == 0 ? 1 : f == 1 ? qb.ext[0] : qb.ext[0] * qb.ext[1];
-            const int nf = f == 0 ? 1 : f == 1 ? nb.ext[0] : nb.ext[0] * nb.ext[1];
+            const int ff = f == 0 ? 1 : f == 1 ? fb.ext[0] : fb.ext[0] * fb.ext[1];
             const long long gf = g.st[f];
             T t1[2], t2[2];
 #pragma unroll
             for (int s = 0; s < 2; ++s) {
               const int o = s ? sf : -sf;
-              const int on = s ? nf : -nf;
+              const int on = s ? ff : -ff;
               const long long go = s ? gf : -gf;
               int cx[3] = {c[0], c[1], c[2]};
               cx[f] += s ? 1 : -1;
-              const T nsum = NU[2 * k * nn + n0 + on] + NU[(2 * k + 1) * nn + n0 + on];
+              T nr2, nl2;
+              nu_at(k, on, cx[f] >= 2 && cx[f] <= g.n[f] - 3, nr2, nl2);
+              const T nsum = nr2 + nl2;
               const T tmp5 = z1(g, cx, d) ? T(0) : (v[o + sd] - v[o - sd]) * (T)0.5 * i1;
               const T tmp6 = tmp5 * nsum * (T)0.25;
               t1[s] = (C.v(L::RHO, idx + go) + C.v(L::RHOB, idx + go)) * tmp6;
@@ -766,20 +790,23 @@ __device__ __forceinline__ void tile_body(const StageArgs &a, const Geo &g, cons
           if (f == d) continue;
           const int k = ks++;
           const T *b = Q + k * nq + r0;
-          const T nr = NU[2 * k * nn + n0], nl = NU[(2 * k + 1) * nn + n0];
+          T nr, nl;
+          nu_at(k, 0, true, nr, nl);
           {  // off-diagonal: B_d -= d_f( (nu_L+nu_R)/2 d_d B_f ), e likewise with B_d
             const int sf = f == 0 ? 1 : f == 1 ? qb.ext[0] : qb.ext[0] * qb.ext[1];
-            const int nf = f == 0 ? 1 : f == 1 ? nb.ext[0] : nb.ext[0] * nb.ext[1];
+            const int ff = f == 0 ? 1 : f == 1 ? fb.ext[0] : fb.ext[0] * fb.ext[1];
             const long long gf = g.st[f];
             T t1[2], t2[2];
 #pragma unroll
             for (int s = 0; s < 2; ++s) {
               const int o = s ? sf : -sf;
-              const int on = s ? nf : -nf;
+              const int on = s ? ff : -ff;
               const long long go = s ? gf : -gf;
               int cx[3] = {c[0], c[1], c[2]};
               cx[f] += s ? 1 : -1;
-              const T nsum = NU[2 * k * nn + n0 + on] + NU[(2 * k + 1) * nn + n0 + on];
+              T nr2, nl2;
+              nu_at(k, on, cx[f] >= 2 && cx[f] <= g.n[f] - 3, nr2, nl2);
+              const T nsum = nr2 + nl2;
               const T tmp2 = z1(g, cx, d) ? T(0) : (b[o + sd] - b[o - sd]) * (T)0.5 * i1;
               t1[s] = tmp2 * nsum * (T)0.5;
               t2[s] = t1[s] * C.v(L::B0 + d, idx + go);
@@ -799,6 +826,11 @@ __device__ __forceinline__ void tile_body(const StageArgs &a, const Geo &g, cons
       }
     }
     __syncthreads();
+  };
+  if (p.hyperdif || p.has_bgb) {
+    dim_pass(std::integral_constant<int, 0>{});
+    dim_pass(std::integral_constant<int, 1>{});
+    if constexpr (D == 3) dim_pass(std::integral_constant<int, 2>{});
   }
 
   stage_epilogue<D, T>(a, g, p, C, c, active, idx, h, dL, numax, red);
@@ -836,10 +868,10 @@ __host__ __device__ constexpr int tile_smem_elems() {
     for (int e = 0; e < D; ++e) {
       n *= ex[e] + (e == dir ? 4 : 0);
       m *= ex[e] + (e == dir ? 6 : 2);
-      u *= ex[e] + (e == dir ? 0 : 2);
+      u *= ex[e] + (e == dir ? 1 : 2);  // face box
     }
     fl = fl > NW * n ? fl : NW * n;
-    qv = qv > NQ * m + 2 * NQ * u ? qv : NQ * m + 2 * NQ * u;
+    qv = qv > NQ * m + NQ * u ? qv : NQ * m + NQ * u;
   }
   return fl > qv ? fl : qv;
 }

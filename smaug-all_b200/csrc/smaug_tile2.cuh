@@ -86,7 +86,12 @@ __device__ __forceinline__ void tile_body2(const StageArgs &a, const Geo &g, con
   const int t = threadIdx.x;
   const int ox = 2 + bx * TX, oy = 2 + by * TY;
   const int n0 = g.n[0], n1 = g.n[1];
-  int c[3] = {ox + t % TX, oy + t / TX, 0};
+  // the cell of this thread.  With 16-wide tiles a warp takes two rows; they
+  // are TY/2 apart rather than adjacent, so that the row offset of the q box
+  // (stride TX + 6 = 22) moves the second half-warp by 16 banks: the q reads
+  // of phase C are free of bank conflicts.
+  constexpr bool PAIRED = TX == 16 && TY == 16;  // 8 rows x 22 = 16 banks mod 32
+  int c[3] = {ox + t % TX, oy + (PAIRED ? ((t >> 4) & 1) * (TY / 2) + (t >> 5) : t / TX), 0};
   const bool active = c[0] <= n0 - 3 && c[1] <= n1 - 3;
   const long long idx = active ? c[0] + (long long)c[1] * g.st[1] : 0;
   const CellT<2, T> C{MIXED ? (const T *)(const void *)a.in32 : (const T *)(const void *)a.in, a.bg, g.N};
