@@ -533,6 +533,8 @@ def main():
     ap.add_argument("--no-blast", action="store_true", help="skip the 3-D blast wave measurements")
     ap.add_argument("--no-atmos3d", action="store_true", help="skip the 3-D stratified atmosphere measurements")
     ap.add_argument("--only-batched", action="store_true", help="just the timed batched run (profiling)")
+    ap.add_argument("--only-blast", action="store_true",
+                    help="just the 3-D blast wave line, printed alone (profiling; --n sets its size)")
     ap.add_argument("--ensemble-count", type=int, default=ENSEMBLE["count"])
     ap.add_argument("--serve-requests", type=int, default=48,
                     help="requests of the serving stream (0: skip); the full stream is 2000")
@@ -545,6 +547,15 @@ def main():
     from smaug_b200 import PREC_FP64, PREC_MIXED, problems
     ctx = Ctx(a)
     W, K = max(3, a.warmup), a.steps
+    if a.only_blast:
+        a.accuracy_steps = 0
+        out = run_blast(a, ctx)
+        if ctx.rank == 0:
+            print(json.dumps({"blast": out}), flush=True)
+        if ctx.dist is not None:
+            ctx.barrier()
+            ctx.dist.destroy_process_group()
+        return 0
     probs = problems.ensemble(a.ensemble_count, seed=ENSEMBLE["seed"] + 1000 * ctx.rank)
     cells = sum(p.interior for p in probs)
 
