@@ -42,6 +42,14 @@ CASES = {
     # non-zero background fields, seeded density perturbation
     "atmos40x20_euler": dict(kind="atmos", n=[40, 20], btype=None, steps=4, rk4=False),
     "atmos40x20_drv_rk4": dict(kind="atmos", n=[40, 20], btype=None, steps=3, rk4=True, driver="const"),
+    # boundary types through the reference's gradops.cu helpers (the shim's
+    # bc_dispatch.inc), loaded ghosts that match no fill rule
+    "ot24_cont_fixed_euler": dict(kind="ot", n=24, btype=[3, 5], steps=5, rk4=False, ghost_noise=True),
+    "ot24_symm_wall_euler": dict(kind="ot", n=24, btype=[6, 6], bmask=[0b10010, 0b100100], steps=5, rk4=False,
+                                 ghost_noise=True),
+    "blast12_asymm_fixed_euler": dict(kind="blast", n=12, btype=[7, 0, 5], steps=3, rk4=False, ghost_noise=True),
+    # divergence-of-B source terms (divb.cu), on a field with a divergence
+    "ot28_divb_euler": dict(kind="ot", n=28, btype=None, steps=5, rk4=False, divb=1, b_noise=True),
 }
 
 
@@ -88,6 +96,24 @@ def make_problem(spec):
         prob = problems.blast_wave(spec["n"])
     if spec.get("btype"):
         prob.btype = tuple(spec["btype"])
+    if spec.get("bmask"):
+        prob.bmask = tuple(spec["bmask"])
+    if spec.get("divb"):
+        prob.divb = 1
+    D = prob.ndim
+    if spec.get("b_noise"):
+        rng = np.random.default_rng(5)
+        for k in range(D):
+            prob.w[2 + D + k] += 0.02 * rng.standard_normal(prob.w.shape[1:])
+    if spec.get("ghost_noise"):
+        ghost = np.zeros(prob.w.shape[1:], dtype=bool)
+        for d in range(D):
+            sl = [slice(None)] * D
+            sl[D - 1 - d] = np.r_[0, 1, prob.n[d] - 2, prob.n[d] - 1]
+            ghost[tuple(sl)] = True
+        rng = np.random.default_rng(21)
+        for f in range(2 + 2 * D):
+            prob.w[f][ghost] *= 1.0 + 0.01 * rng.standard_normal(int(ghost.sum()))
     return prob
 
 
