@@ -137,11 +137,11 @@ def run_reference(a):
     return 0
 
 
-def workload_config(world: int, cells: int | None = None):
-    return {"workload": "batched ensemble: 96 independent 2-D Orszag-Tang vortices, sides {128..768} "
+def workload_config(world: int, cells: int | None = None, count: int = ENSEMBLE["count"]):
+    return {"workload": f"batched ensemble: {count} independent 2-D Orszag-Tang vortices, sides {{128..768}} "
                         "(seed 4242), B0 x U[0.5,1.5], 1% density noise, periodic, RK4, hyperdiffusion on, "
                         "per-simulation dt (reference rule)",
-            "ndim": 2, "simulations": ENSEMBLE["count"], "interior_cells": cells,
+            "ndim": 2, "simulations": count, "interior_cells": cells,
             "parallelism": f"replicas x{world}",
             "l2": "inputs larger than L2: ensemble state > 1 GB"}
 
@@ -598,7 +598,7 @@ def main():
             cpu = {"value": None, "unit": UNIT, "cores": 0, "kind": "reference", "sample": f"failed: {ex}"}
 
     if ctx.rank == 0:
-        cfg = workload_config(ctx.world, cells)
+        cfg = workload_config(ctx.world, cells, a.ensemble_count)
         cfg["precision"] = "mixed: FP32 stage states/stencils; FP64 backgrounds, p_T, e_int, RK base + sum, dt"
         cfg["tile_variant"] = head["tile_variant"]
         line = {
