@@ -28,7 +28,7 @@ struct WorkItem {
 // Tile shapes and occupancy targets (resident blocks per SM the register
 // allocation is made for) the stage kernel is built for; the autotuner picks
 // one.  Variant 0 is the single-simulation default.
-constexpr int kBatchVariants2 = 10;
+constexpr int kBatchVariants2 = 11;
 constexpr int kBatchVariants3 = 6;
 struct BatchVariant {
   int t[3];
@@ -46,6 +46,7 @@ __host__ __device__ inline BatchVariant batch_variant(int D, int v) {
       case 7: return {{32, 8, 1}, 4};
       case 8: return {{16, 16, 1}, 5};
       case 9: return {{16, 8, 1}, 8};
+      case 10: return {{32, 16, 1}, 2};
       default: return {{16, 16, 1}, 2};
     }
   }

@@ -184,14 +184,14 @@ __device__ __forceinline__ void q_all(const CellT<D, T> &c, long long i, int d, 
 // kernel gives the same bits.  b: eb, rho_b, B_b (zeros when the simulation
 // has no energy background).  The maxima are FP32 values and kept in FP32.
 template <int D>
-__device__ __forceinline__ void reduce_cell_mixed(const Geo &g, const Phys &p, const double *o, const double *b,
+__device__ __forceinline__ void reduce_cell_mixed(const Geo &g, const Phys &p, const float *o, const double *b,
                                                   long long idx, float *r) {
   using L = Lay<D>;
-  const float irt = __frcp_rn((float)(o[L::RHO] + b[1]));
+  const float irt = __frcp_rn((float)((double)o[L::RHO] + b[1]));
   float m2 = 0.0f, b2 = 0.0f, bbb = 0.0f, bb2 = 0.0f;
 #pragma unroll
   for (int k = 0; k < D; ++k) {
-    const float m = (float)o[L::M0 + k], bf = (float)o[L::B0 + k], bb = (float)b[2 + k];
+    const float m = o[L::M0 + k], bf = o[L::B0 + k], bb = (float)b[2 + k];
     m2 = __fmaf_rn(m, m, m2);
     b2 = __fmaf_rn(bf, bf, b2);
     bbb = __fmaf_rn(bb, bf, bbb);
@@ -199,7 +199,7 @@ __device__ __forceinline__ void reduce_cell_mixed(const Geo &g, const Phys &p, c
   }
   const float gm1 = (float)(p.gamma - 1.0), gam = (float)p.gamma;
   // p_k = (gamma-1) (e - m^2/(2 rho_t) - B^2/2 - B.B_b)
-  const float ek = __fsub_rn(__fsub_rn(__fsub_rn((float)o[L::EN], __fmul_rn(__fmul_rn(0.5f, m2), irt)),
+  const float ek = __fsub_rn(__fsub_rn(__fsub_rn(o[L::EN], __fmul_rn(__fmul_rn(0.5f, m2), irt)),
                                        __fmul_rn(0.5f, b2)), bbb);
   const float pk = __fmul_rn(gm1, ek);
   // c_s^2 = gamma (p_k + (gamma-1)(e_b - B_b^2/2)) / rho_t
@@ -208,10 +208,10 @@ __device__ __forceinline__ void reduce_cell_mixed(const Geo &g, const Phys &p, c
   const float cf = __fadd_rn(__fmul_rn(__fadd_rn(__fadd_rn(b2, bb2), __fmul_rn(2.0f, bbb)), irt), cs2);
 #pragma unroll
   for (int d = 0; d < D; ++d) {
-    const float bd = (float)(b[2 + d] + o[L::B0 + d]);
+    const float bd = (float)(b[2 + d] + (double)o[L::B0 + d]);
     const float disc = __fsub_rn(__fmul_rn(cf, cf), __fmul_rn(__fmul_rn(__fmul_rn(4.0f, cs2), __fmul_rn(bd, bd)), irt));
     const float cfi = __fmul_rn(0.5f, __fadd_rn(cf, __fsqrt_rn(fmaxf(disc, 0.0f))));
-    const float cff = __fadd_rn(__fsqrt_rn(cfi), fabsf(__fmul_rn((float)o[L::M0 + d], irt)));
+    const float cff = __fadd_rn(__fsqrt_rn(cfi), fabsf(__fmul_rn(o[L::M0 + d], irt)));
     if (cff > r[d] || cff != cff) r[d] = cff;
     if (d == D - 1) {
       const float cour = __fmul_rn(cff, __frcp_rn((float)__ldg(g.dxlast + idx)));
@@ -264,21 +264,21 @@ __device__ __forceinline__ void stage_epilogue(const StageArgs &a, const Geo &g,
       //   c = 1/3, 2/3, 1/3, so A = (S1 + 2 S2 + S3 - 4 W) / 3 as the FP64 path;
       //   stage 4: W <- W + h_4 L_4 + A, kept as value + compensation.
       // Stages 1..3 round to FP32 anyway, so they take the base without c32.
-      double incs[NW];
-#pragma unroll
-      for (int f = 0; f < NW; ++f) incs[f] = h * (double)dL[f];
-      if (p.drv_on) {  // momentum driver with the stage output's density
+      // momentum driver with the stage output's density, added to the
+      // increment of m along drv_dir (dm = 0 without a driver)
+      double dm = 0.0;
+      int dm_f = -1;
+      if (p.drv_on) {
         const double wr = a.kind == 4 ? (double)a.w32[idx] + (double)a.c32[idx] : (double)a.w32[idx];
         const double rb = __ldg(a.bg + (long long)(L::RHOB - NW) * g.N + idx);
-        const double dm = h * driver_vvz<D>(g, p, a.sc, a.tfrac, c) * ((wr + incs[L::RHO]) + rb);
-#pragma unroll
-        for (int k = 0; k < D; ++k)
-          if (k == p.drv_dir) incs[L::M0 + k] += dm;
+        dm = h * driver_vvz<D>(g, p, a.sc, a.tfrac, c) * ((wr + h * (double)dL[L::RHO]) + rb);
+        dm_f = L::M0 + p.drv_dir;
       }
 #pragma unroll
       for (int f = 0; f < NW; ++f) {
         const unsigned j = fo32(f, g.N, idx);
-        const double inc = incs[f];
+        double inc = h * (double)dL[f];
+        if (f == dm_f) inc += dm;
         if (a.kind == 4) {
           const double wn = ((double)a.w32[j] + (double)a.c32[j]) + (inc + (double)a.acc32[j]);
           hi[f] = (float)wn;
@@ -288,7 +288,6 @@ __device__ __forceinline__ void stage_epilogue(const StageArgs &a, const Geo &g,
           const double prev = a.kind == 1 ? 0.0 : (double)a.acc32[j];
           a.acc32[j] = (float)(prev + (a.kind == 2 ? 2.0 : 1.0) * (1.0 / 3.0) * inc);
         }
-        o[f] = (double)hi[f];  // what the next stage reads
       }
     }
     // the cell (its ghost images are written by the ghost pass that follows
@@ -316,7 +315,7 @@ __device__ __forceinline__ void stage_epilogue(const StageArgs &a, const Geo &g,
     for (int b = 0; b < NB; ++b)
       bgv[b] = (b == L::RHOB - NW || p.has_bgb) ? __ldg(a.bg + fo32(b, g.N, (unsigned)idx)) : 0.0;
     if constexpr (MIXED)
-      reduce_cell_mixed<D>(g, p, o, bgv, idx, red);
+      reduce_cell_mixed<D>(g, p, hi, bgv, idx, red);  // what the next stage reads
     else
       reduce_cell<D>(g, p, o, bgv, idx, red);
   }
@@ -459,7 +458,7 @@ __device__ __forceinline__ void ghost_cell(const StageArgs &a, const Geo &g, con
     limit = L0 - 1;
   }
   const long long j = gidx<D>(g, c), src = gidx<D>(g, s);
-  double ov[NW];
+  T ov[NW];
   if (!MIXED) {
 #pragma unroll
     for (int f = 0; f < NW; ++f) {
@@ -478,7 +477,7 @@ __device__ __forceinline__ void ghost_cell(const StageArgs &a, const Geo &g, con
       }
       a.w32[fo32(f, g.N, j)] = v;
       a.c32[fo32(f, g.N, j)] = w;
-      ov[f] = (double)v;
+      ov[f] = v;
     }
   } else {
 #pragma unroll
@@ -486,7 +485,7 @@ __device__ __forceinline__ void ghost_cell(const StageArgs &a, const Geo &g, con
       float v = a.out32[fo32(f, g.N, src)];
       if ((neg >> f) & 1u) v = -v;
       a.out32[fo32(f, g.N, j)] = v;
-      ov[f] = (double)v;
+      ov[f] = v;
     }
   }
   double bgv[NB];

@@ -1,21 +1,22 @@
 // smaug_tile2.cuh -- the 2-D stage body in three phases.
 //
 // Same operator as tile_body (smaug_tile.cuh), reorganised for 2-D so that a
-// tile needs two block barriers instead of ten and computes every per-cell
-// quantity once per tile:
-//   phase A  one balanced loop over the union of three boxes: x-fluxes on the
-//            tile +-2 along x, y-fluxes on the tile +-2 along y, and the six
-//            hyperviscosity inputs q (rho, e_int, v_x, v_y, B_x, B_y) on the
-//            tile +-3 in both dimensions;
+// tile needs two block barriers instead of ten and reads the state from
+// global memory once per cell of the tile +-3:
+//   phase A  the q slots of every cell of the tile +-3 (q_cell: the six
+//            hyperviscosity inputs rho, e_int, v_x, v_y, B_x, B_y, and what
+//            the fluxes and the momentum terms need at the neighbours);
 //   phase B  one loop over runs of cell faces of both dimensions: the ratio
 //            max|d3 q| / max|d1 q| of the hyperviscosity once per face
 //            (nu_R of a cell and nu_L of its right neighbour share their
 //            windows, consecutive faces share their differences), along x on
 //            the tile +-1 in y, along y on the tile +-1 in x (the
 //            off-diagonal terms need nu there);
-//   phase C  per cell: nu = dx c_max c_hyp * ratio on the cell's faces,
-//            divergences, gravity, background energy terms, hyperdiffusion,
-//            then the shared epilogue.
+//   phase C  per cell: the fluxes at the four neighbours along each
+//            dimension from their q slots and their 4th-order divergence,
+//            gravity, background energy terms, hyperdiffusion with
+//            nu = dx c_max c_hyp * ratio on the cell's faces, then the shared
+//            epilogue.
 // A q cell outside the grid along one dimension takes that dimension's pad
 // (0 on the right, q(5) on the left, as the reference's padded copies do);
 // the corners outside both are never read.
@@ -27,21 +28,27 @@
 namespace SMAUG_NS {
 using namespace smaug;
 
-// The q slots of one cell (2-D): the hyperviscosity inputs, slot 0 rho,
-// 1 internal energy (FP64), 2 v_x, 3 v_y, 4 B_x, 5 B_y; then what the
+// The q slots of one cell (2-D).  The hyperviscosity inputs: 0 rho,
+// 1 internal energy (formed in FP64), 2 v_x, 3 v_y, 4 B_x, 5 B_y.  What the
 // momentum terms read at the neighbours: 6 rho_t = rho + rho_b, 7 m_x, 8 m_y.
+// What the fluxes read beyond those: 9 e, 10 the total pressure p_T (formed
+// in FP64, as the reference's pressure recovery), and with an energy
+// background (bgb) 11 B_b,x, 12 B_b,y, 13 e_b (not written without one).
 template <typename T>
-__device__ __forceinline__ void q_cell(const CellT<2, T> &c, long long i, T *q) {
+__device__ __forceinline__ void q_cell(const CellT<2, T> &c, long long i, double gam, bool bgb, T *q) {
   using L = Lay<2>;
   const T rho = c.v(L::RHO, i);
   const double rhob = c.vd(L::RHOB, i);
   const double irtd = 1.0 / ((double)rho + rhob);
   const T irt = (T)irtd;
   const T m0 = c.v(L::M0, i), m1 = c.v(L::M0 + 1, i), b0 = c.v(L::B0, i), b1 = c.v(L::B0 + 1, i);
+  const T e = c.v(L::EN, i);
+  const T bb0 = bgb ? c.v(L::BB0, i) : T(0), bb1 = bgb ? c.v(L::BB0 + 1, i) : T(0);
   const double b2 = (double)b0 * (double)b0 + (double)b1 * (double)b1;
   const double m2 = (double)m0 * (double)m0 + (double)m1 * (double)m1;
+  const double bbb = (double)b0 * (double)bb0 + (double)b1 * (double)bb1;
   q[0] = rho;
-  q[1] = (T)(c.vd(L::EN, i) - 0.5 * (b2 + m2 * irtd));
+  q[1] = (T)((double)e - 0.5 * (b2 + m2 * irtd));
   q[2] = m0 * irt;
   q[3] = m1 * irt;
   q[4] = b0;
@@ -49,39 +56,70 @@ __device__ __forceinline__ void q_cell(const CellT<2, T> &c, long long i, T *q) 
   q[6] = rho + (T)rhob;
   q[7] = m0;
   q[8] = m1;
+  q[9] = e;
+  q[10] = (T)((gam - 1.0) * ((double)e - 0.5 * m2 * irtd) - (gam - 2.0) * (bbb + 0.5 * b2));
+  q[11] = bb0;
+  q[12] = bb1;
+  q[13] = bgb ? c.v(L::EB, i) : T(0);
+}
+
+// The fluxes along dir at the q-box cell r, from its q slots (the physical
+// fluxes of fluxes_at: rho, momentum, energy, induction; B_dir has none):
+// F[0] rho, F[1] m_x, F[2] m_y, F[3] e, F[4] B_f with f the other dimension.
+// In terms of v = m / rho_t, so that no reciprocal is formed here:
+//   m_k:  v_d m_k - b_k (b_d + B_b,d) - B_b,k b_d  (+ p_T on k = d)
+//   e:    v_d (e + e_b + p_T) - (b_d + B_b,d) (b.v) - b_d (B_b.v)
+//   B_f:  v_d (b_f + B_b,f) - (b_d + B_b,d) v_f
+// Explicit FMAs: every build variant gives the same bits.
+template <int dir, int QN, typename T>
+__device__ __forceinline__ void flux_q(const T *Q, int r, bool bgb, T *F) {
+  const T v0 = Q[2 * QN + r], v1 = Q[3 * QN + r], b0 = Q[4 * QN + r], b1 = Q[5 * QN + r];
+  const T m0 = Q[7 * QN + r], m1 = Q[8 * QN + r], e = Q[9 * QN + r], pt = Q[10 * QN + r];
+  T bb0 = 0, bb1 = 0, eb = 0;
+  if (bgb) {
+    bb0 = Q[11 * QN + r];
+    bb1 = Q[12 * QN + r];
+    eb = Q[13 * QN + r];
+  }
+  const T vd = dir == 0 ? v0 : v1, bd = dir == 0 ? b0 : b1, bbd = dir == 0 ? bb0 : bb1;
+  const T bdt = bd + bbd;
+  F[0] = dir == 0 ? m0 : m1;
+  F[1] = vfma(vd, m0, -vfma(b0, bdt, bb0 * bd));
+  F[2] = vfma(vd, m1, -vfma(b1, bdt, bb1 * bd));
+  if (dir == 0)
+    F[1] += pt;
+  else
+    F[2] += pt;
+  const T bv = vfma(b1, v1, b0 * v0), bbv = vfma(bb1, v1, bb0 * v0);
+  F[3] = vfma(vd, (e + eb) + pt, -vfma(bdt, bv, bd * bbv));
+  const T bf = dir == 0 ? b1 : b0, bbf = dir == 0 ? bb1 : bb0, vf = dir == 0 ? v1 : v0;
+  F[4] = vfma(vd, bf + bbf, -(bdt * vf));
 }
 
 // Box sizes of the three-phase body for a TX x TY tile.
 template <typename S>
 struct Box2 {
   static constexpr int TX = S::TX, TY = S::TY;
-  // flux slots: the evolved fields but B_d (its flux along d is zero)
-  static constexpr int NF = Lay<2>::NW - 1;
-  static constexpr int NQS = 9;  // q slots per cell (q_cell)
-  static constexpr int F0X = TX + 4, F0N = F0X * TY;           // x-fluxes: tile +-2 along x
-  static constexpr int F1X = TX, F1N = TX * (TY + 4);          // y-fluxes: tile +-2 along y
-  static constexpr int QX = TX + 6, QN = QX * (TY + 6);        // q: tile +-3
+  static constexpr int NQS = 14;                        // q slots per cell (q_cell)
+  static constexpr int QX = TX + 6, QN = QX * (TY + 6);  // q: tile +-3
   // face ratios along x: faces x+1/2 for x in [-1, TX), rows tile +-1
   static constexpr int V0X = TX + 1, V0N = (TX + 1) * (TY + 2);
   // face ratios along y: faces y+1/2 for y in [-1, TY), columns tile +-1
   static constexpr int V1X = TX + 2, V1N = (TX + 2) * (TY + 1);
   // offsets (elements) of the arrays in shared memory
-  static constexpr int OF0 = 0, OF1 = OF0 + NF * F0N, OQ = OF1 + NF * F1N, OV0 = OQ + NQS * QN, OV1 = OV0 + 5 * V0N;
-  // flux slot of field f along dir
-  static constexpr __host__ __device__ int fslot(int f, int dir) { return f < Lay<2>::B0 + dir ? f : f - 1; }
+  static constexpr int OQ = 0, OV0 = OQ + NQS * QN, OV1 = OV0 + 5 * V0N;
   static constexpr int ELEMS = OV1 + 5 * V1N;
 };
 
 template <typename T, typename S>
 __device__ __forceinline__ void tile_body2(const StageArgs &a, const Geo &g, const Phys &p, int bx, int by, T *sm,
                                            T *red) {
-  constexpr int D = 2;
   using L = Lay<2>;
   using B = Box2<S>;
   constexpr int TX = S::TX, TY = S::TY, NT = TX * TY;
   constexpr int NW = L::NW;
   constexpr bool MIXED = sizeof(T) == sizeof(float);
-  T *F0 = sm + B::OF0, *F1 = sm + B::OF1, *Q = sm + B::OQ, *V0 = sm + B::OV0, *V1 = sm + B::OV1;
+  T *Q = sm + B::OQ, *V0 = sm + B::OV0, *V1 = sm + B::OV1;
 
   const int t = threadIdx.x;
   const int ox = 2 + bx * TX, oy = 2 + by * TY;
@@ -98,49 +136,25 @@ __device__ __forceinline__ void tile_body2(const StageArgs &a, const Geo &g, con
   const double h = a.sc->dt / a.hdiv;
   const T cm[2] = {(T)red_get(a.sc->red[a.red_in], 0), (T)red_get(a.sc->red[a.red_in], 1)};
 
-  // ------------------------------------------------ phase A: fluxes and q
-  // (each branch has its direction as a compile-time constant, so nothing
-  // indexes Geo, cm or the flux temporaries dynamically)
-  auto flux_item = [=](auto dirc, int rr) {
-    constexpr int dir = decltype(dirc)::value;
-    const int cx = dir == 0 ? ox - 2 + rr % B::F0X : ox + rr % B::F1X;
-    const int cy = dir == 0 ? oy + rr / B::F0X : oy - 2 + rr / B::F1X;
-    T F[NW];
-    if (cx >= 0 && cx < n0 && cy >= 0 && cy < n1) {
-      fluxes_fast<2, T>(C, cx + (long long)cy * g.st[1], dir, p.gamma, p.has_bgb, F);
+  // ------------------------------------------------ phase A: q on the tile +-3
+  for (int rr = t; rr < B::QN; rr += NT) {
+    int cx = ox - 3 + rr % B::QX, cy = oy - 3 + rr / B::QX;
+    T q[B::NQS];
+    const bool inx = cx >= 0 && cx < n0, iny = cy >= 0 && cy < n1;
+    // pads of the padded copies: right 0, left q(5); corners never read
+    // (slots 6..13 are read at the tile +-2 along one dimension only, always
+    // inside the grid)
+    if ((!inx && !iny) || cx >= n0 || cy >= n1) {
+#pragma unroll
+      for (int k = 0; k < B::NQS; ++k) q[k] = 0;
     } else {
-#pragma unroll
-      for (int f = 0; f < NW; ++f) F[f] = 0;
+      if (cx < 0) cx = 5;
+      if (cy < 0) cy = 5;
+      q_cell<T>(C, cx + (long long)cy * g.st[1], p.gamma, p.has_bgb, q);
     }
-    T *dst = (dir == 0 ? F0 : F1) + rr;
-    constexpr int stride = dir == 0 ? B::F0N : B::F1N;
 #pragma unroll
-    for (int f = 0; f < NW; ++f)
-      if (f != L::B0 + dir) dst[B::fslot(f, dir) * stride] = F[f];
-  };
-  for (int r = t; r < B::F0N + B::F1N + B::QN; r += NT) {
-    if (r < B::F0N) {
-      flux_item(std::integral_constant<int, 0>{}, r);
-    } else if (r < B::F0N + B::F1N) {
-      flux_item(std::integral_constant<int, 1>{}, r - B::F0N);
-    } else {
-      const int rr = r - B::F0N - B::F1N;
-      int cx = ox - 3 + rr % B::QX, cy = oy - 3 + rr / B::QX;
-      T q[B::NQS];
-      const bool inx = cx >= 0 && cx < n0, iny = cy >= 0 && cy < n1;
-      // pads of the padded copies: right 0, left q(5); corners never read
-      // (slots 6..8 are read at the tile +-1 only, always inside the grid)
-      if ((!inx && !iny) || cx >= n0 || cy >= n1) {
-#pragma unroll
-        for (int k = 0; k < B::NQS; ++k) q[k] = 0;
-      } else {
-        if (cx < 0) cx = 5;
-        if (cy < 0) cy = 5;
-        q_cell<T>(C, cx + (long long)cy * g.st[1], q);
-      }
-#pragma unroll
-      for (int k = 0; k < B::NQS; ++k) Q[k * B::QN + rr] = q[k];
-    }
+    for (int k = 0; k < B::NQS; ++k)
+      if (k < 11 || p.has_bgb) Q[k * B::QN + rr] = q[k];
   }
   __syncthreads();
 
@@ -212,21 +226,30 @@ __device__ __forceinline__ void tile_body2(const StageArgs &a, const Geo &g, con
   if (active) {
     const int tx = c[0] - ox, ty = c[1] - oy;
     const T idx1[2] = {(T)(1.0 / __ldg(g.dx1[0] + c[0])), (T)(1.0 / __ldg(g.dx1[1] + c[1]))};
-    // flux divergences
-#pragma unroll
-    for (int dir = 0; dir < 2; ++dir) {
-      if (z4(g, c, dir)) continue;
-      const T *Fb = dir == 0 ? F0 + (tx + 2) + B::F0X * ty : F1 + tx + B::F1X * (ty + 2);
-      const int st = dir == 0 ? 1 : B::F1X;
-      const int fs = dir == 0 ? B::F0N : B::F1N;
+    const int r0 = (tx + 3) + B::QX * (ty + 3);
+    // flux divergences: -(8 (F_+1 - F_-1) - (F_+2 - F_-2)) / (12 dx), the
+    // fluxes of the neighbours (inside the grid: the cell is an inner cell)
+    // from their q slots
+    auto div_terms = [&](auto dc) {
+      constexpr int dir = decltype(dc)::value;
+      if (z4(g, c, dir)) return;
+      constexpr int sd = dir == 0 ? 1 : B::QX;
       const T w12 = idx1[dir] * (T)(1.0 / 12.0);
+      T Fp[5], Fm[5], d1[5];
+      flux_q<dir, B::QN>(Q, r0 + sd, p.has_bgb, Fp);
+      flux_q<dir, B::QN>(Q, r0 - sd, p.has_bgb, Fm);
 #pragma unroll
-      for (int f = 0; f < NW; ++f) {
-        if (f == L::B0 + dir) continue;  // zero flux
-        const T *Fp = Fb + B::fslot(f, dir) * fs;
-        dL[f] -= ((T)8 * (Fp[st] - Fp[-st]) - (Fp[2 * st] - Fp[-2 * st])) * w12;
+      for (int k = 0; k < 5; ++k) d1[k] = Fp[k] - Fm[k];
+      flux_q<dir, B::QN>(Q, r0 + 2 * sd, p.has_bgb, Fp);
+      flux_q<dir, B::QN>(Q, r0 - 2 * sd, p.has_bgb, Fm);
+#pragma unroll
+      for (int k = 0; k < 5; ++k) {
+        const int f = k < 4 ? k : L::B0 + 1 - dir;
+        dL[f] = vfma(-vfma((T)8, d1[k], -(Fp[k] - Fm[k])), w12, dL[f]);
       }
-    }
+    };
+    div_terms(std::integral_constant<int, 0>{});
+    div_terms(std::integral_constant<int, 1>{});
     // gravity
     if (p.has_grav) {
       const T rho = C.v(L::RHO, idx), irt = (T)(1.0 / ((double)rho + C.vd(L::RHOB, idx)));
@@ -237,7 +260,6 @@ __device__ __forceinline__ void tile_body2(const StageArgs &a, const Geo &g, con
       }
     }
     if (p.divb) divb_sources<T>(C, g, p, c, idx, dL);
-    const int r0 = (tx + 3) + B::QX * (ty + 3);
     // the terms along dimension d (a compile-time constant in each call, so
     // that nothing indexes Geo, c, cm or idx1 dynamically)
     auto dim_terms = [&](auto dc) {

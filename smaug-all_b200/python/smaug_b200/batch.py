@@ -101,7 +101,7 @@ class Batch:
         v = ctypes.c_int(-1)
         ms = (ctypes.c_double * 16)()
         self._check(self.lib.smaug_batch_tune(self.h, reps, ctypes.byref(v), ms, 16), "smaug_batch_tune")
-        nv = 10 if self.ndim == 2 else 6
+        nv = 11 if self.ndim == 2 else 6
         return v.value, list(ms[:nv])
 
     def set_variant(self, v: int):

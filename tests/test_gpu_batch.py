@@ -50,7 +50,7 @@ def test_batch_matches_single_simulation(need_gpu, precision):
 def test_batch_tile_shapes_and_graph_replay_are_identical(need_gpu):
     probs = ot_mix()[:3]
     ref = [alone(p, 21, PREC_MIXED)[0] for p in probs]
-    for v in range(10):
+    for v in range(11):
         b = Batch(2, precision=PREC_MIXED, arena_bytes=256 << 20, max_sims=4)
         slots = [b.add(p, 21) for p in probs]
         b.set_variant(v)

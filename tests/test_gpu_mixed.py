@@ -61,7 +61,15 @@ def test_mixed_vs_oracle(need_gpu, kind, n, steps, dt_mode, dt0):
     assert err.max() <= MIXED_RTOL, err
     # the FP32 path really is a different computation, not the FP64 one
     assert err.max() > 0.0
-    assert abs(eng.scalars()["dt"] - o.dt) <= 1e-5 * o.dt
+    # Under the dt rule with hyperdiffusion on, dt is the viscous limit. It is
+    # inversely proportional to the largest hyperviscosity coefficient, i.e. to
+    # max|d3 q| / max|d1 q| with q in FP32. Rounding q (6e-8 relative) puts up
+    # to 8 x 6e-8 |q| into a third difference of size (k dx)^3 |q| ~ 3e-3 |q|
+    # on a 48^2 Orszag-Tang grid: 1.6e-4 relative. The Courant limit carries
+    # only the wave speeds' FP32 rounding.
+    viscous = dt_mode == 1 and prob.hyperdif and o.s.dtdiffvisc == o.dt
+    dt_rtol = 2e-4 if viscous else 1e-5
+    assert abs(eng.scalars()["dt"] - o.dt) <= dt_rtol * o.dt
 
 
 def test_mixed_blast_500_steps_fixed_dt(need_gpu):
