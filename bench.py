@@ -330,7 +330,10 @@ def run_e2e_batched(probs, prec, ctx, steps):
     from smaug_b200 import Batch, footprint
     cells = sum(p.interior for p in probs)
     fp = sum(footprint(p, prec) for p in probs)
+    # host inputs, as a user holds them: each simulation's state and metric
+    # in pinned memory
     ins = [torch.from_numpy(np.ascontiguousarray(p.w)).pin_memory() for p in probs]
+    mets = [torch.from_numpy(np.concatenate([a.ravel() for a in p.delx()])).pin_memory() for p in probs]
     outs = [torch.empty_like(t).pin_memory() for t in ins]
     b = Batch(2, precision=prec, arena_bytes=int(fp * 1.02) + (64 << 20), max_sims=len(probs), device=ctx.local)
     stream = torch.cuda.ExternalStream(b.stream)
@@ -338,7 +341,7 @@ def run_e2e_batched(probs, prec, ctx, steps):
     torch.cuda.synchronize()
 
     def job():
-        slots = [b.add(p, steps, w=t.numpy()) for p, t in zip(probs, ins)]
+        slots = [b.add(p, steps, w=t.numpy(), delx=m.numpy()) for p, t, m in zip(probs, ins, mets)]
         b.step(steps)
         for sl, o in zip(slots, outs):
             b.state(sl, out=o.numpy())
@@ -347,8 +350,9 @@ def run_e2e_batched(probs, prec, ctx, steps):
     b.close()
     ms_max = ctx.max_ms(ms)
     nbytes = sum(t.numel() * 8 for t in ins)
+    mbytes = sum(m.numel() * 8 for m in mets) // probs[0].ndim  # the last dim's metric is copied
     return {"value": ctx.world * cells * steps / (ms_max / 1e3), "unit": UNIT,
-            "h2d_bytes_per_step": nbytes / steps, "d2h_bytes_per_step": nbytes / steps}
+            "h2d_bytes_per_step": (nbytes + mbytes) / steps, "d2h_bytes_per_step": nbytes / steps}
 
 
 def accuracy_study(prob, steps: int, device: int):

@@ -248,7 +248,8 @@ __global__ void combine_kernel(const float *__restrict__ hi, const float *__rest
 // cells, from a host metric (ndim * N doubles).  Returns an error or nullptr.
 const char *metric_host(const SimPlan &r, const double *delx, double *d1, double minsq[3]) {
   const int D = r.D;
-  const long long N = r.geo.N;
+  const long long N = r.geo.N, K = r.geo.K;
+  const int n0 = r.geo.n[0], n1 = r.geo.n[1], n2 = D == 3 ? r.geo.n[2] : 1;
   size_t off = 0;
   for (int d = 0; d < 3; ++d) minsq[d] = INFINITY;
   for (int d = 0; d < D; ++d) {
@@ -259,23 +260,26 @@ const char *metric_host(const SimPlan &r, const double *delx, double *d1, double
       c[d] = x;
       d1[off + x] = m[c[0] + c[1] * r.geo.st[1] + c[2] * r.geo.st[2]];
     }
-    for (long long j = 0; j < N; ++j) {
-      long long q = j;
-      int c[3];
-      c[0] = (int)(q % r.geo.n[0]);
-      q /= r.geo.n[0];
-      c[1] = (int)(q % r.geo.n[1]);
-      c[2] = (int)(q / r.geo.n[1]);
-      bool inner = true;
-      for (int e = 0; e < D; ++e)
-        if (c[e] < 2 || c[e] > r.geo.n[e] - 3) inner = false;
-      if (inner && m[j] != d1[off + c[d]]) return "metric is not a tensor-product grid on the inner cells";
-      if (!(m[j] > 0.0)) return "metric entries must be positive";
-      if (j < r.geo.K) {
-        const double v = (m[j]) * (m[j]);
-        if (v < minsq[d]) minsq[d] = v;
+    // one pass in storage order (x fastest): inner cells must match the
+    // line, every entry must be positive, the first K cells give min delx^2
+    const double *line = d1 + off;
+    double mn = INFINITY;
+    long long j = 0;
+    for (int z = 0; z < n2; ++z) {
+      const bool zin = D < 3 || (z >= 2 && z <= n2 - 3);
+      for (int y = 0; y < n1; ++y) {
+        const bool yzin = zin && y >= 2 && y <= n1 - 3;
+        const double lyz = d == 1 ? line[y] : line[z];  // the line value when d != 0
+        for (int x = 0; x < n0; ++x, ++j) {
+          const double v = m[j];
+          if (yzin && x >= 2 && x <= n0 - 3 && v != (d == 0 ? line[x] : lyz))
+            return "metric is not a tensor-product grid on the inner cells";
+          if (!(v > 0.0)) return "metric entries must be positive";
+          if (j < K && v * v < mn) mn = v * v;
+        }
       }
     }
+    minsq[d] = mn;
     off += n;
   }
   return nullptr;

@@ -45,11 +45,17 @@ class Batch:
             msg = self.lib.smaug_batch_last_error(self.h).decode() if self.h else ""
             raise SmaugError(f"{what} failed ({rc}): {msg}")
 
-    def add(self, prob, nsteps: int, dt_mode: int = 1, dt0: float = 0.0, w=None) -> int | None:
+    def add(self, prob, nsteps: int, dt_mode: int = 1, dt0: float = 0.0, w=None, delx=None) -> int | None:
         """Admit a simulation; its slot, or None when the batch is full.  w:
-        the initial state (default prob.w), e.g. a view of pinned memory."""
+        the initial state (default prob.w), e.g. a view of pinned memory;
+        delx: the metric, ndim grid-shaped arrays back to back (default
+        prob.delx())."""
         p = make_params(prob, rk4=True, dt_mode=dt_mode, dt0=dt0, precision=self.precision)
-        delx = _f64(np.concatenate([a.ravel() for a in prob.delx()]))
+        if delx is None:
+            delx = np.concatenate([a.ravel() for a in prob.delx()])
+        delx = _f64(delx)
+        if delx.size != prob.ndim * prob.w[0].size:
+            raise SmaugError("metric size does not match the problem")
         w = _f64(prob.w if w is None else w)
         if w.size != prob.w.size:
             raise SmaugError("state size does not match the problem")
