@@ -331,9 +331,9 @@ int smaug_batch_add(smaug_batch *b, const smaug_params *prm, const double *delx,
   if (p.mixed != b->mixed) return bfail(b, SMAUG_ERR_ARG, "simulation precision differs from the batch's");
   if (!p.rk4 || p.exact) return bfail(b, SMAUG_ERR_ARG, "batch simulations use rk4 = 1 and exact = 0");
   const long long N = p.geo.N;
+  // one line per dim here; the metric itself is checked on the device below
   std::vector<double> d1(p.geo.n[0] + p.geo.n[1] + p.geo.n[2]);
-  double minsq[3];
-  if (const char *m = metric_host(p, delx, d1.data(), minsq)) return bfail(b, SMAUG_ERR_ARG, m);
+  metric_lines_host(p, delx, d1.data());
   int slot = -1;
   for (int i = 0; i < b->max_inst; ++i)
     if (!b->slots[i].used) {
@@ -365,15 +365,11 @@ int smaug_batch_add(smaug_batch *b, const smaug_params *prm, const double *delx,
     for (auto &f : I.F) f = (float *)take(sizeof(float) * p.NW * N);
   else
     for (int k = 1; k < 4; ++k) I.W[k] = (double *)take(sizeof(double) * p.NW * N);
-  // backgrounds: are the energy background terms live?
-  int has = 0;
   const double *bh = w + (size_t)N * p.NW;
-  for (long long j = 0; j < N && !has; ++j) {
-    if (bh[j] != 0.0) has = 1;
-    for (int k = 0; k < p.D; ++k)
-      if (bh[(size_t)(2 + k) * N + j] != 0.0) has = 1;
-  }
-  p.phys.has_bgb = has;
+  // Whether the energy background terms are live is found on the device
+  // (bg_scan_kernel) and set after the load; the load's initial maxima read
+  // the backgrounds either way (zeros give the same values).
+  p.phys.has_bgb = 1;
   size_t o1 = 0;
   for (int d = 0; d < p.D; ++d) {
     p.geo.dx1[d] = dx1 + o1;
@@ -391,20 +387,27 @@ int smaug_batch_add(smaug_batch *b, const smaug_params *prm, const double *delx,
   I.sc = sc;
   I.active = 1;
   cudaStream_t s = b->stream;
+  // The full metric goes to a stage buffer that nothing uses before the
+  // first step (mixed F[2]: NW >= 2 D floats per cell; FP64 W[1]) for its
+  // check; the last dim's array stays as dxlast.
+  double *mscratch = p.mixed ? (double *)(void *)I.F[2] : I.W[1];
   BK(cudaMemsetAsync(sc, 0, sizeof(DevScalars), s));
-  BK(cudaMemcpyAsync(sc->minsq, minsq, sizeof(minsq), cudaMemcpyHostToDevice, s));
   BK(cudaMemcpyAsync(dx1, d1.data(), sizeof(double) * d1.size(), cudaMemcpyHostToDevice, s));
   BK(cudaMemcpyAsync(drv, drv_host.data(), sizeof(double) * drv_host.size(), cudaMemcpyHostToDevice, s));
-  BK(cudaMemcpyAsync(dxlast, delx + (size_t)(p.D - 1) * N, sizeof(double) * N, cudaMemcpyHostToDevice, s));
+  BK(cudaMemcpyAsync(mscratch, delx, sizeof(double) * p.D * N, cudaMemcpyHostToDevice, s));
+  BK(cudaMemcpyAsync(dxlast, mscratch + (size_t)(p.D - 1) * N, sizeof(double) * N, cudaMemcpyDeviceToDevice, s));
   BK(cudaMemcpyAsync(I.W[0], w, sizeof(double) * p.NW * N, cudaMemcpyHostToDevice, s));
   BK(cudaMemcpyAsync(bg, bh, sizeof(double) * p.NB * N, cudaMemcpyHostToDevice, s));
   ghost_fill(I.W[0], p.NW, p.geo, p.D, s);
   const double dt0 = p.phys.dt_mode == 1 ? (p.dt0 > 0 ? p.dt0 : 1.0e-8) : p.dt0;
-  one_reset_kernel<<<1, 1, 0, s>>>(sc, dt0);
+  one_reset_kernel<<<1, 1, 0, s>>>(sc, dt0);  // status 0
+  minsq_init_kernel<<<1, 1, 0, s>>>(sc);
+  metric_kernel<<<b->sms * 4, 256, 0, s>>>(mscratch, p.geo, p.D, nullptr, sc);
+  bg_scan_kernel<<<b->sms * 4, 256, 0, s>>>(bg, N, p.D, sc);
   smaug_fast::launch_reduce(p.D, I.W[0], bg, p.geo, p.phys, &sc->red[0], s, 0);
   if (p.geo.has_const) smaug_fast::launch_reduce(p.D, I.W[0], bg, p.geo, p.phys, &sc->floor, s, 1);
   if (p.mixed) split_kernel<<<148 * 8, 256, 0, s>>>(I.W[0], I.F[0], I.F[1], (long long)p.NW * N);
-  b->launches += p.D + 2 + (p.mixed ? 1 : 0) + (p.geo.has_const ? 1 : 0);
+  b->launches += p.D + 5 + (p.mixed ? 1 : 0) + (p.geo.has_const ? 1 : 0);
   BK(cudaGetLastError());
   if (p.geo.has_const) {  // fixed boundaries: every stage buffer holds the loaded ghosts
     const size_t n = (size_t)p.NW * N;
@@ -416,10 +419,20 @@ int smaug_batch_add(smaug_batch *b, const smaug_params *prm, const double *delx,
         BK(cudaMemcpyAsync(I.W[k], I.W[0], sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
     }
   }
+  int chk[2] = {0, 0};  // metric status, live background
+  BK(cudaMemcpyAsync(&chk[0], &sc->status, sizeof(int), cudaMemcpyDeviceToHost, s));
+  BK(cudaMemcpyAsync(&chk[1], &sc->bg_live, sizeof(int), cudaMemcpyDeviceToHost, s));
+  BK(cudaStreamSynchronize(s));  // the sources above are host temporaries
+  if (chk[0] != 0) {
+    arena_free(b, off, fp);
+    return bfail(b, SMAUG_ERR_ARG, "metric is not a tensor-product grid on the inner cells, or has a non-positive entry");
+  }
+  p.phys.has_bgb = chk[1];
+  I.phys = p.phys;
   BK(cudaMemcpyAsync(b->d_left + slot, &nsteps, sizeof(long long), cudaMemcpyHostToDevice, s));
   const int zero = 0;
   BK(cudaMemcpyAsync(b->d_status + slot, &zero, sizeof(int), cudaMemcpyHostToDevice, s));
-  BK(cudaStreamSynchronize(s));  // the sources above are host temporaries
+  BK(cudaStreamSynchronize(s));
   Slot &S = b->slots[slot];
   S.used = true;
   S.off = off;

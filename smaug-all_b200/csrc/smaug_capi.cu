@@ -242,52 +242,6 @@ cudaError_t run_steps(Run &r, int nsteps) {
   return cudaSuccess;
 }
 
-// Device-side metric set-up for smaug_step_noalloc, whose metric already sits
-// in device memory: the 1-D metric of each dim along an inner line, a
-// tensor-product check on the inner cells (status flag), and the minimum of
-// delx_d^2 over the first K cells as an order-preserving atomic minimum on the
-// bit patterns of positive doubles (minsq must start at +inf).
-__global__ void metric_kernel(const double *delx, Geo g, int D, double *dx1, DevScalars *sc) {
-  const long long tid = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  const long long nthr = (long long)gridDim.x * blockDim.x;
-  long long off = 0;
-  for (int d = 0; d < D; ++d) {
-    for (long long x = tid; x < g.n[d]; x += nthr) {
-      int c[3] = {2, 2, D == 3 ? 2 : 0};
-      c[d] = (int)x;
-      dx1[off + x] = delx[(long long)d * g.N + c[0] + c[1] * g.st[1] + c[2] * g.st[2]];
-    }
-    off += g.n[d];
-  }
-  for (long long j = tid; j < g.N; j += nthr) {
-    long long q = j;
-    int c[3];
-    c[0] = (int)(q % g.n[0]);
-    q /= g.n[0];
-    c[1] = (int)(q % g.n[1]);
-    c[2] = (int)(q / g.n[1]);
-    bool inner = true;
-    for (int e = 0; e < D; ++e)
-      if (c[e] < 2 || c[e] > g.n[e] - 3) inner = false;
-    for (int d = 0; d < D; ++d) {
-      const double v = delx[(long long)d * g.N + j];
-      if (!(v > 0.0)) atomicExch(&sc->status, (int)SMAUG_ERR_ARG);
-      if (inner) {
-        int cl[3] = {2, 2, D == 3 ? 2 : 0};
-        cl[d] = c[d];
-        if (v != delx[(long long)d * g.N + cl[0] + cl[1] * g.st[1] + cl[2] * g.st[2]])
-          atomicExch(&sc->status, (int)SMAUG_ERR_ARG);
-      }
-      if (j < g.K) atomicMin((unsigned long long *)&sc->minsq[d], (unsigned long long)__double_as_longlong(v * v));
-    }
-  }
-}
-
-__global__ void minsq_init_kernel(DevScalars *sc) {
-  if (threadIdx.x == 0 && blockIdx.x == 0)
-    for (int d = 0; d < 3; ++d) sc->minsq[d] = INFINITY;
-}
-
 }  // namespace
 
 struct smaug_ctx {
@@ -422,20 +376,18 @@ static int load_state(smaug_ctx *ctx, const double *w, size_t count, cudaMemcpyK
   const Phys before = r.phys;
   CK(cudaMemcpyAsync(r.W[0], w, sizeof(double) * N * r.NW, kind, r.stream));
   CK(cudaMemcpyAsync(r.bg, w + (size_t)N * r.NW, sizeof(double) * N * r.NB, kind, r.stream));
-  // host-side scan of the backgrounds: are the energy background terms live?
-  if (kind == cudaMemcpyHostToDevice) {
-    int has = 0;
-    const double *b = w + (size_t)N * r.NW;
-    for (long long j = 0; j < N && !has; ++j) {
-      if (b[j] != 0.0) has = 1;  // eb
-      for (int k = 0; k < r.D; ++k)
-        if (b[(size_t)(2 + k) * N + j] != 0.0) has = 1;
-    }
-    r.phys.has_bgb = has;
-  } else {
-    r.phys.has_bgb = 1;
-  }
+  // Are the energy background terms live?  Found on the device after the
+  // copy; the load's initial maxima read the backgrounds either way (zeros
+  // give the same values).
+  r.phys.has_bgb = 1;
   CK(run_load(r));
+  CK(cudaMemsetAsync(&r.sc->bg_live, 0, sizeof(int), r.stream));
+  bg_scan_kernel<<<148 * 4, 256, 0, r.stream>>>(r.bg, N, r.D, r.sc);
+  r.launches++;
+  int live = 1;
+  CK(cudaMemcpyAsync(&live, &r.sc->bg_live, sizeof(int), cudaMemcpyDeviceToHost, r.stream));
+  CK(cudaStreamSynchronize(r.stream));
+  r.phys.has_bgb = live;
   CK(run_upload_inst(r));
   CK(cudaStreamSynchronize(r.stream));
   ctx->have_state = true;

@@ -246,20 +246,31 @@ __global__ void combine_kernel(const float *__restrict__ hi, const float *__rest
 
 // 1-D metric lines, tensor-product check and min delx^2 over the first K
 // cells, from a host metric (ndim * N doubles).  Returns an error or nullptr.
+// The 1-D metric of each dim along an inner line (n0 + n1 + n2 doubles).
+void metric_lines_host(const SimPlan &r, const double *delx, double *d1) {
+  const int D = r.D;
+  size_t off = 0;
+  for (int d = 0; d < D; ++d) {
+    const double *m = delx + (size_t)d * r.geo.N;
+    for (int x = 0; x < r.geo.n[d]; ++x) {
+      int c[3] = {2, 2, D == 3 ? 2 : 0};
+      c[d] = x;
+      d1[off + x] = m[c[0] + c[1] * r.geo.st[1] + c[2] * r.geo.st[2]];
+    }
+    off += r.geo.n[d];
+  }
+}
+
 const char *metric_host(const SimPlan &r, const double *delx, double *d1, double minsq[3]) {
   const int D = r.D;
   const long long N = r.geo.N, K = r.geo.K;
   const int n0 = r.geo.n[0], n1 = r.geo.n[1], n2 = D == 3 ? r.geo.n[2] : 1;
+  metric_lines_host(r, delx, d1);
   size_t off = 0;
   for (int d = 0; d < 3; ++d) minsq[d] = INFINITY;
   for (int d = 0; d < D; ++d) {
     const double *m = delx + (size_t)d * N;
     const int n = r.geo.n[d];
-    for (int x = 0; x < n; ++x) {
-      int c[3] = {2, 2, D == 3 ? 2 : 0};
-      c[d] = x;
-      d1[off + x] = m[c[0] + c[1] * r.geo.st[1] + c[2] * r.geo.st[2]];
-    }
     // one pass in storage order (x fastest): inner cells must match the
     // line, every entry must be positive, the first K cells give min delx^2
     const double *line = d1 + off;
@@ -303,6 +314,65 @@ void driver_lines(const SimPlan &r, const smaug_params *prm, double *out) {
     }
     off += n;
   }
+}
+
+// Device-side metric set-up, for a metric in device memory: the 1-D metric of
+// each dim along an inner line (into dx1, unless it is null), a tensor-product
+// check on the inner cells and a positivity check (status = SMAUG_ERR_ARG on a
+// failure), and the minimum of delx_d^2 over the first K cells as an
+// order-preserving atomic minimum on the bit patterns of positive doubles
+// (minsq must start at +inf).  Cell indices fit 31 bits (plan_sim).
+__global__ void metric_kernel(const double *delx, Geo g, int D, double *dx1, DevScalars *sc) {
+  const long long tid = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  const long long nthr = (long long)gridDim.x * blockDim.x;
+  long long off = 0;
+  for (int d = 0; d < D && dx1; ++d) {
+    for (long long x = tid; x < g.n[d]; x += nthr) {
+      int c[3] = {2, 2, D == 3 ? 2 : 0};
+      c[d] = (int)x;
+      dx1[off + x] = delx[(long long)d * g.N + c[0] + c[1] * g.st[1] + c[2] * g.st[2]];
+    }
+    off += g.n[d];
+  }
+  const unsigned n0 = (unsigned)g.n[0], n1 = (unsigned)g.n[1];
+  for (long long j = tid; j < g.N; j += nthr) {
+    unsigned q = (unsigned)j;
+    int c[3];
+    c[0] = (int)(q % n0);
+    q /= n0;
+    c[1] = (int)(q % n1);
+    c[2] = (int)(q / n1);
+    bool inner = true;
+    for (int e = 0; e < D; ++e)
+      if (c[e] < 2 || c[e] > g.n[e] - 3) inner = false;
+    for (int d = 0; d < D; ++d) {
+      const double v = delx[(long long)d * g.N + j];
+      if (!(v > 0.0)) atomicExch(&sc->status, (int)SMAUG_ERR_ARG);
+      if (inner) {
+        int cl[3] = {2, 2, D == 3 ? 2 : 0};
+        cl[d] = c[d];
+        if (v != delx[(long long)d * g.N + cl[0] + cl[1] * g.st[1] + cl[2] * g.st[2]])
+          atomicExch(&sc->status, (int)SMAUG_ERR_ARG);
+      }
+      if (j < g.K) atomicMin((unsigned long long *)&sc->minsq[d], (unsigned long long)__double_as_longlong(v * v));
+    }
+  }
+}
+
+__global__ void minsq_init_kernel(DevScalars *sc) {
+  if (threadIdx.x == 0 && blockIdx.x == 0)
+    for (int d = 0; d < 3; ++d) sc->minsq[d] = INFINITY;
+}
+
+// Is the energy background live (a nonzero e_b or B_b anywhere)?  OR-ed
+// into sc->bg_live, which the caller clears first.
+__global__ void bg_scan_kernel(const double *__restrict__ bg, long long N, int D, DevScalars *sc) {
+  int any = 0;
+  for (long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x; j < N; j += (long long)gridDim.x * blockDim.x) {
+    any |= bg[j] != 0.0;  // e_b
+    for (int k = 0; k < D; ++k) any |= bg[(2 + k) * N + j] != 0.0;  // B_b
+  }
+  if (__syncthreads_or(any) && threadIdx.x == 0) atomicOr(&sc->bg_live, 1);
 }
 
 }  // namespace

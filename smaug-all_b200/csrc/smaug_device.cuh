@@ -37,7 +37,7 @@ struct DevScalars {
   int step;
   int status;
   int go;         // batch only: this simulation takes the current step
-  int pad_;
+  int bg_live;    // set on load: the state has a nonzero energy background (e_b, B_b)
   double t;       // simulation time at the start of the current step (driver)
   Reduce red[5];  // [0] state at step start, [1..3] RK stage outputs, [4] state at step end
   // maxima over the ghost cells that keep their loaded values (fixed
