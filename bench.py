@@ -605,6 +605,8 @@ def main():
         cfg = workload_config(ctx.world, cells, a.ensemble_count)
         cfg["precision"] = "mixed: FP32 stage states/stencils; FP64 backgrounds, p_T, e_int, RK base + sum, dt"
         cfg["tile_variant"] = head["tile_variant"]
+        # the autotuner's RK stage-1 time of every tile variant on this batch
+        cfg["tile_variant_stage1_ms"] = [round(m, 4) for m in head["tune_stage1_ms"]]
         line = {
             "metric": METRIC, "value": head["value"], "unit": UNIT, "n_gpus": ctx.world, "steps": K,
             "warmup": W, "ms_per_step": head["ms_per_step"], "higher_is_better": True,

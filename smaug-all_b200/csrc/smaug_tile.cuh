@@ -183,6 +183,18 @@ __device__ __forceinline__ void q_all(const CellT<D, T> &c, long long i, int d, 
 // rounded operations, never contracted: every build variant of the stage
 // kernel gives the same bits.  b: eb, rho_b, B_b (zeros when the simulation
 // has no energy background).  The maxima are FP32 values and kept in FP32.
+//
+// A fast pass comes first. It takes the square roots and the metric's
+// reciprocal from the hardware approximations (x rsqrtf(x), __fdividef); every
+// other operation is the same as in the exact pass. That puts each approximate
+// speed within about 8 ulp (1e-6 relative) of its correctly rounded value: the
+// terms under the roots are identical, and the sums after them add
+// non-negative terms. If every approximate speed of the cell stays more than
+// 1e-5 below the thread's running maximum, the cell cannot raise it and is
+// done. Any other cell, a NaN included, takes the correctly rounded pass. The
+// maxima come out the same bits either way.
+__device__ __forceinline__ float sqrt_approx(float x) { return x > 0.0f ? x * rsqrtf(x) : 0.0f; }
+
 template <int D>
 __device__ __forceinline__ void reduce_cell_mixed(const Geo &g, const Phys &p, const float *o, const double *b,
                                                   long long idx, float *r) {
@@ -206,6 +218,26 @@ __device__ __forceinline__ void reduce_cell_mixed(const Geo &g, const Phys &p, c
   const float pbg = __fmul_rn(gm1, __fsub_rn((float)b[0], __fmul_rn(0.5f, bb2)));
   const float cs2 = __fmul_rn(__fmul_rn(gam, __fadd_rn(pk, pbg)), irt);
   const float cf = __fadd_rn(__fmul_rn(__fadd_rn(__fadd_rn(b2, bb2), __fmul_rn(2.0f, bbb)), irt), cs2);
+  {
+    constexpr float kBelow = 1.0f - 1e-5f;
+    const float rdx = __fdividef(1.0f, (float)__ldg(g.dxlast + idx));
+    bool need = false;
+#pragma unroll
+    for (int d = 0; d < D; ++d) {
+      const float bd = (float)(b[2 + d] + (double)o[L::B0 + d]);
+      const float disc =
+          __fsub_rn(__fmul_rn(cf, cf), __fmul_rn(__fmul_rn(__fmul_rn(4.0f, cs2), __fmul_rn(bd, bd)), irt));
+      const float cfi = __fmul_rn(0.5f, __fadd_rn(cf, sqrt_approx(fmaxf(disc, 0.0f))));
+      const float cff = __fadd_rn(sqrt_approx(cfi), fabsf(__fmul_rn(o[L::M0 + d], irt)));
+      need |= !(cff < r[d] * kBelow);
+      if (d == D - 1) {
+        const float cour = cff * rdx;
+        need |= !(cour < r[3] * kBelow);
+        if (idx >= g.K) need |= !(cour < r[4] * kBelow);
+      }
+    }
+    if (!need) return;
+  }
 #pragma unroll
   for (int d = 0; d < D; ++d) {
     const float bd = (float)(b[2 + d] + (double)o[L::B0 + d]);

@@ -111,6 +111,53 @@ struct Box2 {
   static constexpr int ELEMS = OV1 + 5 * V1N;
 };
 
+// The rows of the tile that the epilogue reads are prefetched toward L2 at the start
+// of the tile, so that their DRAM latency overlaps phases A-C. Those rows are the
+// cell's RK base, the accumulator and the compensation where the stage reads them,
+// rho_b and the energy backgrounds, and the last dim's metric. Each (array, row)
+// segment of TX cells gets a prefetch at its first and its last byte. Every address
+// lies in its array: the rows are inner rows, and a row's TX cells from ox run at
+// most into the next row.
+template <typename T, int TX, int TY, int NT>
+__device__ __forceinline__ void prefetch_epilogue_rows(const StageArgs &a, const Geo &g, const Phys &p, int ox,
+                                                       int oy) {
+  using L = Lay<2>;
+  constexpr int NW = L::NW;
+  constexpr bool MIXED = sizeof(T) == sizeof(float);
+  const int nrow = min(TY, g.n[1] - 2 - oy);
+  const bool acc = MIXED ? a.kind >= 2 : (a.kind == 3 || a.kind == 4);
+  const bool comp = MIXED && a.kind == 4;
+  // arrays: base 0..NW-1, accumulator NW..2NW-1, compensation 2NW..3NW-1,
+  // backgrounds 3NW..3NW+3 (rho_b always), the last dim's metric 3NW+4
+  constexpr int NA = 3 * NW + 5;
+  for (int s = threadIdx.x; s < NA * TY; s += NT) {
+    const int arr = s / TY, row = s % TY;
+    if (row >= nrow) continue;
+    const unsigned cell = (unsigned)(ox + (oy + row) * g.st[1]);
+    const char *ptr = nullptr;
+    int es = (int)sizeof(T);
+    if (arr < NW) {
+      ptr = MIXED ? (const char *)(a.w32 + fo32(arr, g.N, cell)) : (const char *)(a.base + fo32(arr, g.N, cell));
+    } else if (arr < 2 * NW) {
+      if (acc)
+        ptr = MIXED ? (const char *)(a.acc32 + fo32(arr - NW, g.N, cell))
+                    : (const char *)(a.acc + fo32(arr - NW, g.N, cell));
+    } else if (arr < 3 * NW) {
+      if (comp) ptr = (const char *)(a.c32 + fo32(arr - 2 * NW, g.N, cell));
+    } else if (arr < 3 * NW + 4) {
+      const int b = arr - 3 * NW;
+      if (b == L::RHOB - NW || p.has_bgb) ptr = (const char *)(a.bg + fo32(b, g.N, cell));
+      es = 8;
+    } else {
+      ptr = (const char *)(g.dxlast + cell);
+      es = 8;
+    }
+    if (!ptr) continue;
+    asm volatile("prefetch.global.L2 [%0];" ::"l"(ptr));
+    asm volatile("prefetch.global.L2 [%0];" ::"l"(ptr + TX * es - 1));
+  }
+}
+
 template <typename T, typename S>
 __device__ __forceinline__ void tile_body2(const StageArgs &a, const Geo &g, const Phys &p, int bx, int by, T *sm,
                                            T *red) {
@@ -135,6 +182,7 @@ __device__ __forceinline__ void tile_body2(const StageArgs &a, const Geo &g, con
   const CellT<2, T> C{MIXED ? (const T *)(const void *)a.in32 : (const T *)(const void *)a.in, a.bg, g.N};
   const double h = a.sc->dt / a.hdiv;
   const T cm[2] = {(T)red_get(a.sc->red[a.red_in], 0), (T)red_get(a.sc->red[a.red_in], 1)};
+  prefetch_epilogue_rows<T, TX, TY, NT>(a, g, p, ox, oy);
 
   // ------------------------------------------------ phase A: q on the tile +-3
   for (int rr = t; rr < B::QN; rr += NT) {
