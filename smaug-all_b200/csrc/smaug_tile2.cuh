@@ -158,9 +158,44 @@ __device__ __forceinline__ void prefetch_epilogue_rows(const StageArgs &a, const
   }
 }
 
+// The q box of tile (nbx, nby) of the same simulation (the block's next work
+// item), prefetched toward L2: the stage input's fields and the backgrounds that
+// q_cell reads, one prefetch per line of each row segment of the box, clamped to
+// the grid.
+template <typename T, int TX, int TY, int NT>
+__device__ __forceinline__ void prefetch_qbox_rows(const StageArgs &a, const Geo &g, const Phys &p, int nbx,
+                                                   int nby) {
+  using L = Lay<2>;
+  constexpr int NW = L::NW;
+  constexpr bool MIXED = sizeof(T) == sizeof(float);
+  const int x0 = max(2 + nbx * TX - 3, 0), x1 = min(2 + nbx * TX + TX + 2, g.n[0] - 1);
+  const int y0 = max(2 + nby * TY - 3, 0), y1 = min(2 + nby * TY + TY + 2, g.n[1] - 1);
+  const int nrow = y1 - y0 + 1;
+  // arrays: the stage input's NW fields, then rho_b, e_b, B_b
+  constexpr int NA = NW + 4;
+  for (int s = threadIdx.x; s < NA * (TY + 6); s += NT) {
+    const int arr = s / (TY + 6), row = s % (TY + 6);
+    if (row >= nrow) continue;
+    const unsigned c0 = (unsigned)(x0 + (y0 + row) * g.st[1]), c1 = (unsigned)(x1 + (y0 + row) * g.st[1]);
+    const char *p0, *p1;
+    if (arr < NW) {
+      const T *in = MIXED ? (const T *)(const void *)a.in32 : (const T *)(const void *)a.in;
+      p0 = (const char *)(in + fo32(arr, g.N, c0));
+      p1 = (const char *)(in + fo32(arr, g.N, c1));
+    } else {
+      const int b = arr - NW;
+      if (!(b == L::RHOB - NW || p.has_bgb)) continue;
+      p0 = (const char *)(a.bg + fo32(b, g.N, c0));
+      p1 = (const char *)(a.bg + fo32(b, g.N, c1));
+    }
+    asm volatile("prefetch.global.L2 [%0];" ::"l"(p0));
+    asm volatile("prefetch.global.L2 [%0];" ::"l"(p1));
+  }
+}
+
 template <typename T, typename S>
-__device__ __forceinline__ void tile_body2(const StageArgs &a, const Geo &g, const Phys &p, int bx, int by, T *sm,
-                                           T *red) {
+__device__ __forceinline__ void tile_body2(const StageArgs &a, const Geo &g, const Phys &p, int bx, int by, int nbx,
+                                           int nby, T *sm, T *red) {
   using L = Lay<2>;
   using B = Box2<S>;
   constexpr int TX = S::TX, TY = S::TY, NT = TX * TY;
@@ -183,6 +218,7 @@ __device__ __forceinline__ void tile_body2(const StageArgs &a, const Geo &g, con
   const double h = a.sc->dt / a.hdiv;
   const T cm[2] = {(T)red_get(a.sc->red[a.red_in], 0), (T)red_get(a.sc->red[a.red_in], 1)};
   prefetch_epilogue_rows<T, TX, TY, NT>(a, g, p, ox, oy);
+  if (nbx >= 0) prefetch_qbox_rows<T, TX, TY, NT>(a, g, p, nbx, nby);
 
   // ------------------------------------------------ phase A: q on the tile +-3
   for (int rr = t; rr < B::QN; rr += NT) {
