@@ -239,7 +239,10 @@ int smaug_batch_destroy(smaug_batch *b);
  * Admit a simulation: prm as for smaug_create (ndim and precision those of
  * the batch), delx as for smaug_set_metric, w as for smaug_set_state (host
  * buffers, copied before the call returns), nsteps = RK4 steps to take.
- * Returns SMAUG_ERR_FULL when no slot or no arena block is free.
+ * Returns SMAUG_ERR_FULL when no slot or no arena block is free, and
+ * SMAUG_ERR_ARG for a metric that is not a tensor-product grid on the inner
+ * cells or has a non-positive entry (checked on the device, in the slot's own
+ * memory, which is released again).
  */
 int smaug_batch_add(smaug_batch *b, const smaug_params *prm, const double *delx, const double *w,
                     long long nsteps, int *slot);
