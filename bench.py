@@ -262,8 +262,9 @@ def measure(eng, n_int, steps, warmup, ctx, sample_clocks):
             "launches": launches, "clocks": clocks, "avg_stage_ms": st_ms / max(st_n, 1)}
 
 
-def run_batched(probs, prec, ctx, steps, warmup, sample_clocks):
-    """The whole ensemble in one batch: tune, warm up, time `steps` steps."""
+def run_batched(probs, prec, ctx, steps, warmup, sample_clocks, force_variant=-1):
+    """The whole ensemble in one batch: tune (or take force_variant), warm up,
+    time `steps` steps."""
     import torch
 
     from smaug_b200 import Batch, footprint
@@ -275,6 +276,9 @@ def run_batched(probs, prec, ctx, steps, warmup, sample_clocks):
         if b.add(p, warmup + steps + extra) is None:
             raise RuntimeError("ensemble does not fit its arena")
     variant, tune_ms = b.tune(reps=3)
+    if force_variant >= 0:  # profiling one tile variant
+        b.set_variant(force_variant)
+        variant = force_variant
     stream = torch.cuda.ExternalStream(b.stream)
     b.step(warmup)
     b.sync()
@@ -540,6 +544,8 @@ def main():
     ap.add_argument("--only-blast", action="store_true",
                     help="just the 3-D blast wave line, printed alone (profiling; --n sets its size)")
     ap.add_argument("--ensemble-count", type=int, default=ENSEMBLE["count"])
+    ap.add_argument("--variant", type=int, default=-1,
+                    help="tile variant of the batched mixed run (default: the autotuner's choice)")
     ap.add_argument("--serve-requests", type=int, default=48,
                     help="requests of the serving stream (0: skip); the full stream is 2000")
     ap.add_argument("--accuracy-steps", type=int, default=50,
@@ -563,7 +569,7 @@ def main():
     probs = problems.ensemble(a.ensemble_count, seed=ENSEMBLE["seed"] + 1000 * ctx.rank)
     cells = sum(p.interior for p in probs)
 
-    head = run_batched(probs, PREC_MIXED, ctx, K, W, sample_clocks=True)
+    head = run_batched(probs, PREC_MIXED, ctx, K, W, sample_clocks=True, force_variant=a.variant)
     line_extra = {}
     if not a.only_batched:
         line_extra["batched_fp64"] = {k: v for k, v in run_batched(probs, PREC_FP64, ctx, K, W, False).items()
