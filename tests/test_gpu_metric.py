@@ -56,3 +56,32 @@ def test_bad_metric_is_rejected_and_frees_nothing(need_gpu, kind, defect):
     b.step(2)
     assert np.isfinite(b.state(s)).all()
     b.close()
+
+
+@pytest.mark.parametrize("kind", ["ot", "blast"])
+@pytest.mark.parametrize("defect", ["inner", "nonpositive_ghost", "count"])
+def test_set_metric_rejects_a_bad_metric(need_gpu, kind, defect):
+    """smaug_set_metric checks the metric on the host, in one pass in storage
+    order: SMAUG_ERR_ARG, and the context keeps its metric and still steps
+    to the same bits as a context that never saw the bad one."""
+    import ctypes
+
+    from smaug_b200 import Engine
+    prob = problems.orszag_tang(24) if kind == "ot" else problems.blast_wave(10, seed=2)
+    D = prob.ndim
+    m = [a.copy() for a in prob.delx()]
+    if defect == "inner":
+        m[D - 1][(3,) * D] *= 1.0 + 1e-12
+    elif defect == "nonpositive_ghost":
+        m[0][(0,) * D] = -1.0
+    flat = np.ascontiguousarray(np.concatenate([a.ravel() for a in m]))
+    count = flat.size - (1 if defect == "count" else 0)
+    e = Engine(prob, rk4=True, precision=PREC_MIXED)
+    rc = e.lib.smaug_set_metric(e.h, flat.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), count)
+    assert rc != 0
+    e.step(2)
+    ref = Engine(prob, rk4=True, precision=PREC_MIXED)
+    ref.step(2)
+    assert np.array_equal(e.state(), ref.state())
+    e.close()
+    ref.close()
