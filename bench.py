@@ -149,43 +149,63 @@ def workload_config(world: int, cells: int | None = None, count: int = ENSEMBLE[
 # ----------------------------------------------------------------- GPU side
 
 class ClockSampler:
-    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+    FIELDS = ("timestamp,index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
     def __init__(self, device: int):
         self.device = device
         self.proc = None
-        self.path = ROOT / "gpurun_out" / f"clocks_rank{device}.csv"
+        # the raw samples (the line carries their summary): SMAUG_CLOCKS_DIR, else
+        # the system's temporary directory
+        import tempfile
+        out = Path(os.environ.get("SMAUG_CLOCKS_DIR", tempfile.gettempdir()))
+        self.path = out / f"smaug_clocks_rank{device}.csv"
 
     def start(self):
         try:
-            self.path.parent.mkdir(exist_ok=True)
+            self.path.parent.mkdir(parents=True, exist_ok=True)
             self.f = open(self.path, "w")
-            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
-                                          "--format=csv,noheader,nounits", "-lms", "100"],
+            # line-buffered where stdbuf exists: no sample is lost in a buffer
+            # when the sampler is stopped
+            import shutil
+            pre = ["stdbuf", "-oL"] if shutil.which("stdbuf") else []
+            self.proc = subprocess.Popen(pre + ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
+                                                "--format=csv,noheader,nounits", "-lms", "100"],
                                          stdout=self.f, stderr=subprocess.DEVNULL)
         except Exception:
             self.proc = None
 
-    def stop(self):
+    def stop(self, t_on: float | None = None, t_off: float | None = None):
+        """Summary of the samples taken between host times t_on and t_off (one
+        sampling period of slack each side; the first sample after t_on when
+        none falls inside)."""
+        import datetime
         if not self.proc:
             return None
-        self.proc.terminate()
+        import signal
+        self.proc.send_signal(signal.SIGINT)  # nvidia-smi ends its loop cleanly on SIGINT
         try:
             self.proc.wait(timeout=5)
         except Exception:
             self.proc.kill()
+            self.proc.wait()
         self.f.close()
-        rows = []
+        rows, later = [], []
         for line in self.path.read_text().splitlines():
             parts = [x.strip() for x in line.split(",")]
-            if len(parts) < 9:
+            if len(parts) < 10:
                 continue
             try:
-                rows.append((float(parts[1]), float(parts[2]), parts[5:9]))
+                ts = datetime.datetime.strptime(parts[0], "%Y/%m/%d %H:%M:%S.%f").timestamp()
+                row = (float(parts[2]), float(parts[3]), parts[6:10])
             except ValueError:
                 continue
+            if t_on is None or t_on - 0.1 <= ts <= t_off + 0.1:
+                rows.append(row)
+            elif ts > t_on:
+                later.append(row)
+        rows = rows or later[:1]
         if not rows:
             return None
         sm = sorted(r[0] for r in rows)
@@ -275,6 +295,11 @@ def run_batched(probs, prec, ctx, steps, warmup, sample_clocks, force_variant=-1
     for p in probs:
         if b.add(p, warmup + steps + extra) is None:
             raise RuntimeError("ensemble does not fit its arena")
+    # the clock sampler starts before the autotuner, so that it is sampling
+    # when the timed region starts; only the samples inside that region count
+    sampler = ClockSampler(ctx.local) if sample_clocks else None
+    if sampler:
+        sampler.start()
     variant, tune_ms = b.tune(reps=3)
     if force_variant >= 0:  # profiling one tile variant
         b.set_variant(force_variant)
@@ -282,16 +307,15 @@ def run_batched(probs, prec, ctx, steps, warmup, sample_clocks, force_variant=-1
     stream = torch.cuda.ExternalStream(b.stream)
     b.step(warmup)
     b.sync()
-    sampler = ClockSampler(ctx.local) if sample_clocks else None
-    if sampler:
-        sampler.start()
     ctx.barrier()
     torch.cuda.synchronize()
+    t_on = time.time()
     l0 = b.launches
     ms = event_ms(stream, lambda: b.step(steps))
     b.sync()
+    t_off = time.time()
     ctx.barrier()
-    clocks = sampler.stop() if sampler else None
+    clocks = sampler.stop(t_on, t_off) if sampler else None
     launches = b.launches - l0
     ms_max = ctx.max_ms(ms)
     b.profile_stages(True)
