@@ -37,14 +37,26 @@ sys.path.insert(0, str(ROOT / "smaug-all_b200" / "python"))
 
 METRIC = "cell-updates/s: batched mixed-prec vs plain FP64, 1 B200; p50/p99 latency"
 UNIT = "cell-updates/s"
-# algorithmic HBM bytes per cell-update (one cell, one full RK4 step), 3-D:
-# FP64: 14 evolved-field passes x 8 fields x 8 B + 4 background passes x 5 x 8 B
-BYTES_PER_CELL_UPDATE_FP64_3D = (14 * 8 + 4 * 5) * 8  # 1056 B
-# mixed: 19 FP32 evolved-field passes x 8 fields x 4 B + 4 FP64 background passes
-BYTES_PER_CELL_UPDATE_MIXED_3D = 19 * 8 * 4 + 4 * 5 * 8  # 768 B
-# 2-D (6 evolved fields, 4 backgrounds): FP64 800 B, mixed 584 B
-BYTES_PER_CELL_UPDATE_FP64_2D = (14 * 6 + 4 * 4) * 8
-BYTES_PER_CELL_UPDATE_MIXED_2D = 19 * 6 * 4 + 4 * 4 * 8
+# Algorithmic HBM bytes per cell-update (one inner cell, one full RK4 step):
+# the fused one-pass-per-stage minimum of SAC's fourstep, 14 evolved-field
+# accesses (stage 1 reads U writes U1; 2 reads U1, U writes U2; 3 reads U2, U,
+# U1 writes U3, U1'; 4 reads U3, U, U1' writes U) of NW fields plus 4 reads of
+# the NB FP64 background fields: 14 NW s + 4 NB 8 bytes, s the state's element
+# size (8 in FP64, 4 in the mixed path's FP32 states).
+def alg_bytes_per_cell_update(ndim: int, mixed: bool) -> int:
+    nw, nb = 2 + 2 * ndim, 2 + ndim
+    return 14 * nw * (4 if mixed else 8) + 4 * nb * 8
+
+
+BYTES_PER_CELL_UPDATE_FP64_2D = alg_bytes_per_cell_update(2, False)   # 800 B
+BYTES_PER_CELL_UPDATE_MIXED_2D = alg_bytes_per_cell_update(2, True)   # 464 B
+BYTES_PER_CELL_UPDATE_FP64_3D = alg_bytes_per_cell_update(3, False)   # 1056 B
+BYTES_PER_CELL_UPDATE_MIXED_3D = alg_bytes_per_cell_update(3, True)   # 608 B
+# What this design moves per cell-update in the mixed path (its traffic, not
+# the algorithmic minimum): the RK base is an FP32 value plus an FP32
+# compensation and the increment sum is an FP32 buffer, 19 FP32 field passes
+# in all: 2-D 584 B, 3-D 768 B.
+DESIGN_BYTES_MIXED = {2: 19 * 6 * 4 + 4 * 4 * 8, 3: 19 * 8 * 4 + 4 * 5 * 8}
 ENSEMBLE = {"count": 96, "seed": 4242}
 SAMPLE_N = 128         # CPU sample: one 128^2 Orszag-Tang simulation of the ensemble per process
 SAMPLE_SUBSTEPS = 4    # reference single steps per RK4-equivalent step
@@ -155,6 +167,15 @@ class ClockSampler:
 
     def __init__(self, device: int):
         self.device = device
+        # nvidia-smi numbers GPUs physically and ignores CUDA_VISIBLE_DEVICES:
+        # select this process's device by its UUID
+        self.uuid = None
+        try:
+            import torch
+            u = str(torch.cuda.get_device_properties(device).uuid)
+            self.uuid = u if u.startswith("GPU-") else "GPU-" + u
+        except Exception:
+            pass
         self.proc = None
         # the raw samples (the line carries their summary): SMAUG_CLOCKS_DIR, else
         # the system's temporary directory
@@ -170,7 +191,8 @@ class ClockSampler:
             # when the sampler is stopped
             import shutil
             pre = ["stdbuf", "-oL"] if shutil.which("stdbuf") else []
-            self.proc = subprocess.Popen(pre + ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
+            sel = self.uuid or str(self.device)
+            self.proc = subprocess.Popen(pre + ["nvidia-smi", "-i", sel, f"--query-gpu={self.FIELDS}",
                                                 "--format=csv,noheader,nounits", "-lms", "100"],
                                          stdout=self.f, stderr=subprocess.DEVNULL)
         except Exception:
@@ -211,7 +233,8 @@ class ClockSampler:
         sm = sorted(r[0] for r in rows)
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         reasons = sorted({names[i] for r in rows for i, v in enumerate(r[2]) if v.lower().startswith("active")})
-        return {"sm_mhz": sm[len(sm) // 2], "sm_max_mhz": rows[0][1], "reasons": reasons, "samples": len(rows)}
+        return {"sm_mhz": sm[len(sm) // 2], "sm_max_mhz": rows[0][1], "reasons": reasons, "samples": len(rows),
+                "gpu": self.uuid}
 
 
 def event_ms(stream, fn):
@@ -443,6 +466,7 @@ def run_blast(a, ctx):
                      "roofline": {"achieved": ach, "peak": peak, "frac": ach / peak, "unit": "GB/s",
                                   "alg_bytes_per_launch": alg}}
         if name == "mixed":
+            out[name]["roofline"]["design_bytes_per_launch"] = DESIGN_BYTES_MIXED[3] / 4 * n_int
             # every step: smaug_set_state from pinned host memory, smaug_step,
             # smaug_get_state and smaug_get_scalars back to the host
             dptr = ctypes.POINTER(ctypes.c_double)
@@ -614,6 +638,7 @@ def main():
         e2e = None
 
     alg = BYTES_PER_CELL_UPDATE_MIXED_2D / 4 * cells
+    design = DESIGN_BYTES_MIXED[2] / 4 * cells
     achieved = alg / (head["avg_stage_ms"] / 1e3) / 1e9
     peak, peak_kind = load_peaks()
     tr = load_traffic()
@@ -643,7 +668,11 @@ def main():
             "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic", "config": cfg,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic, "peak_source": peak_kind,
-                         "kernel": kernel, "avg_launch_ms": head["avg_stage_ms"], "alg_bytes_per_launch": alg},
+                         "kernel": kernel, "avg_launch_ms": head["avg_stage_ms"], "alg_bytes_per_launch": alg,
+                         "alg_bytes_basis": "464 B per cell-update / 4 stages (14 x 6 FP32 state + 4 x 4 FP64 "
+                                            "background accesses per inner cell per RK4 step)",
+                         "design_bytes_per_launch": design,
+                         "design_frac": design / (head["avg_stage_ms"] / 1e3) / 1e9 / peak},
             "cpu_baseline": cpu,
             "e2e": e2e,
             "gpu_launches": head["launches"],

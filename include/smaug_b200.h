@@ -202,10 +202,15 @@ int smaug_stage_times(smaug_ctx *ctx, double *ms_total, long long *count);
  * counters cleared); the scratch keeps the previous call's contents, so calls
  * whose work overlaps on the GPU (different streams, other threads) race on
  * it and must be serialised by the caller.  The first call on a device looks
- * up the scratch address (cudaGetSymbolAddress); make that first call before
- * any stream capture.  The call waits for its stream before returning;
- * scalars_out (8 doubles, as smaug_get_scalars, may be NULL) and err (may be
- * NULL) are host buffers.  FP64 only: precision must be SMAUG_PREC_FP64.
+ * up the scratch address (cudaGetSymbolAddress).  Every call blocks: it
+ * checks the metric on the device and waits for that check before it writes
+ * anything (a bad metric returns SMAUG_ERR_ARG with w_out untouched, also
+ * when w_out == w_in), copies small tables from host memory, and waits for
+ * its stream before returning.  So it must not be called while its stream,
+ * or (in global capture mode) any stream of the calling thread, is being
+ * captured into a CUDA graph.  scalars_out (8 doubles, as smaug_get_scalars,
+ * may be NULL) and err (may be NULL) are host buffers.  FP64 only: precision
+ * must be SMAUG_PREC_FP64.
  */
 #define SMAUG_NOALLOC_SCRATCH_BYTES (32u << 20)
 int smaug_step_noalloc(const smaug_params *prm, const double *delx_dev, const double *w_in_dev,

@@ -29,7 +29,7 @@ _PI = ctypes.POINTER(_I)
 def build_oracle(force: bool = False) -> Path:
     src = HERE / "smaug_oracle.c"
     if force or not LIB.exists() or LIB.stat().st_mtime < src.stat().st_mtime:
-        subprocess.run(["gcc", "-O2", "-ffp-contract=off", "-fPIC", "-shared", "-o", str(LIB),
+        subprocess.run(["gcc", "-O2", "-ffp-contract=off", "-fopenmp", "-fPIC", "-shared", "-o", str(LIB),
                         str(src), "-lm"], check=True)
     return LIB
 

@@ -266,15 +266,79 @@ def build(reference: Path, variants=("2d", "3d", "2d_drv"), jobs: int = 8) -> No
         if r.returncode != 0:
             raise RuntimeError(f"link failed:\n{r.stderr[-4000:]}")
         print(f"built {lib}")
+    build_hydro(reference)
+
+
+# The hydrostatic-background helpers of the reference's spicule model
+# (models/initialisation_user.h.spicule1_mpi): inte() (326-343), the trapezoid
+# rule of its pressure integral, and temp() (345-360), its tanh temperature
+# profile.  The two functions are cut out of the model file as they stand and
+# compiled with a minimal prelude of the types they use, behind two extern "C"
+# wrappers, into oracle/_ref/libsmaug_ref_hydro.so.
+HYDRO_MODEL = "../models/initialisation_user.h.spicule1_mpi"
+HYDRO_FUNCS = (r"^real\s+inte\s*\(", r"^void\s+temp\s*\(")
+HYDRO_PRELUDE = """#include <math.h>
+typedef double real;
+struct params { int n[3]; };
+enum { pos1 = 0 };
+/* positions of the first coordinate along dim 0, one row (the only use) */
+#define encode3_uin(p, i, j, k, f) ((f) * (p)->n[0] + (i))
+"""
+HYDRO_WRAP = """
+extern "C" double ref_inte(const double *col, int n, int i, double dx) {
+  real **w = new real *[n];
+  for (int k = 0; k < n; ++k) w[k] = const_cast<real *>(col + k);
+  const double r = inte(w, n, i, 0, dx);
+  delete[] w;
+  return r;
+}
+extern "C" void ref_temp(const double *z, int n, double *T) {
+  struct params p = {{n, 1, 1}};
+  int ii[3] = {0, 0, 0};
+  temp(nullptr, const_cast<real *>(z), ii, &p, T);
+}
+"""
+
+
+def build_hydro(reference: Path) -> Path:
+    src = (reference / "dev" / "smaug" / "src" / HYDRO_MODEL).resolve().read_text(errors="replace")
+    parts = [HYDRO_PRELUDE]
+    for pat in HYDRO_FUNCS:
+        m = re.search(pat, src, re.M)
+        if not m:
+            raise RuntimeError(f"{pat} not found in {HYDRO_MODEL}")
+        close = _match_brace(src, src.index("{", m.end() - 1))
+        parts.append(src[m.start():close + 1] + "\n")
+    parts.append(HYDRO_WRAP)
+    d = OUT / "buildhydro"
+    d.mkdir(parents=True, exist_ok=True)
+    cpp = d / "hydro_ref.cpp"
+    cpp.write_text("".join(parts))
+    lib = OUT / "libsmaug_ref_hydro.so"
+    cmd = ["g++", "-O2", "-ffp-contract=off", "-fPIC", "-shared", "-w", "-o", str(lib), str(cpp), "-lm"]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"hydro build failed:\n{r.stderr[-4000:]}")
+    print(f"built {lib}")
+    return lib
 
 
 def main() -> int:
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default=os.environ.get("SMAUG_REFERENCE", "/root/reference"))
+    ap.add_argument("--reference", default=None,
+                    help="reference source tree (default: $SMAUG_REFERENCE, else ../reference beside the repo)")
     ap.add_argument("--jobs", type=int, default=os.cpu_count() or 4)
     ap.add_argument("--variants", default=",".join(VARIANTS))
     a = ap.parse_args()
-    build(Path(a.reference), tuple(a.variants.split(",")), a.jobs)
+    if a.reference is None:
+        sys.path.insert(0, str(HERE.parents[1]))
+        from oracle.ref_shim import reference_root
+        ref = reference_root()
+        if ref is None:
+            ap.error("reference sources not found: pass --reference or set SMAUG_REFERENCE")
+    else:
+        ref = Path(a.reference)
+    build(ref, tuple(a.variants.split(",")), a.jobs)
     return 0
 
 

@@ -10,8 +10,11 @@
  * file agrees with the host build of the reference (oracle/ref_shim) to the
  * last bits.  Paths below are relative to dev/smaug/ of the reference.
  *
- * Build: gcc -O2 -ffp-contract=off -fPIC -shared (no FMA contraction, as the
- * reference host build).
+ * Build: gcc -O2 -ffp-contract=off -fopenmp -fPIC -shared (no FMA contraction,
+ * as the reference host build).  The per-cell loops run under OpenMP: every
+ * iteration writes only its own cell, and the maxima are taken per thread and
+ * then combined with the same comparison, so the results do not depend on the
+ * thread count (max is exact).
  */
 #include "smaug_oracle.h"
 
@@ -170,6 +173,7 @@ static double cfast_of(const sm_oracle_grid *g, const lay_t *L, const double *w,
 void sm_oracle_cfast(const sm_oracle_grid *g, const double *w, int dim, double *cf) {
   lay_t L0 = mklay(g);
   const lay_t *L = &L0;
+#pragma omp parallel for schedule(static)
   for (long i = 0; i < L->N; ++i) cf[i] = cfast_of(g, L, w, i, dim);
 }
 
@@ -180,9 +184,16 @@ void sm_oracle_cmax(const sm_oracle_grid *g, const double *w, double *cmax) {
   const lay_t *L = &L0;
   for (int d = 0; d < L->D; ++d) {
     double m = 0.0;
-    for (long i = 0; i < L->N; ++i) {
-      double v = cfast_of(g, L, w, i, d);
-      if (v > m) m = v;
+#pragma omp parallel
+    {
+      double ml = 0.0;
+#pragma omp for schedule(static) nowait
+      for (long i = 0; i < L->N; ++i) {
+        double v = cfast_of(g, L, w, i, d);
+        if (v > ml) ml = v;
+      }
+#pragma omp critical
+      if (ml > m) m = ml;
     }
     cmax[d] = m;
   }
@@ -209,9 +220,16 @@ double sm_oracle_select_dt(const sm_oracle_grid *g, const double *w, int step, s
    * every call, so only the last dimension's c_fast/dx survives the dim loop. */
   double *cour = (double *)malloc(sizeof(double) * L->N);
   double maxc = 0.0;
-  for (long i = 0; i < L->N; ++i) {
-    cour[i] = cfast_of(g, L, w, i, dl) / (g->delx[dl][i]);
-    if (cour[i] > maxc) maxc = cour[i];
+#pragma omp parallel
+  {
+    double ml = 0.0;
+#pragma omp for schedule(static) nowait
+    for (long i = 0; i < L->N; ++i) {
+      cour[i] = cfast_of(g, L, w, i, dl) / (g->delx[dl][i]);
+      if (cour[i] > ml) ml = cour[i];
+    }
+#pragma omp critical
+    if (ml > maxc) maxc = ml;
   }
   s->maxcourant = maxc;
   if (((g->courant) / (maxc)) > 1.0e-8) s->dt = (g->courant) / (maxc); /* iosmaug.cpp:874-875 */
@@ -298,6 +316,12 @@ static double qat(const lay_t *L, const double *q, long idx, const int c[3], int
 static void hyperviscosity(const sm_oracle_grid *g, const lay_t *L, const double *q, int field, int d,
                            double cmax, double *nur, double *nul, double *numax) {
   const double chyp = g->chyp[field];
+  double numax_all = *numax;
+#pragma omp parallel
+  {
+  double numax_l = 0.0;
+  double *numax = &numax_l; /* this thread's maximum, combined below */
+#pragma omp for schedule(static) nowait
   for (long idx = 0; idx < L->N; ++idx) {
     int c[3];
     coords(L, idx, c);
@@ -335,6 +359,10 @@ static void hyperviscosity(const sm_oracle_grid *g, const lay_t *L, const double
     if (nur[idx] > *numax) *numax = nur[idx];
     if (nul[idx] > *numax) *numax = nul[idx];
   }
+#pragma omp critical
+  if (numax_l > numax_all) numax_all = numax_l;
+  }
+  *numax = numax_all;
 }
 
 /* ------------------------------------------------------------ boundaries */
@@ -384,6 +412,8 @@ void sm_oracle_boundary(const sm_oracle_grid *g, double *w) {
       const long s = L->st[d];
       int type = g->btype[d];
       if (type == 6 && ((g->bmask[d] >> f) & 1)) type = 7;
+      /* the sources of this pass are inner along d: no cell is both read and written */
+#pragma omp parallel for schedule(static)
       for (long idx = 0; idx < L->N; ++idx) {
         int c[3];
         coords(L, idx, c);
@@ -434,6 +464,7 @@ static void divb_terms(const sm_oracle_grid *g, const lay_t *L, const double *wi
   const long N = L->N;
   const int NW = L->NW;
   double *dw = (double *)calloc((size_t)NW * N, sizeof(double));
+#pragma omp parallel for schedule(static)
   for (long idx = 0; idx < N; ++idx) {
     int c[3];
     coords(L, idx, c);
@@ -451,6 +482,7 @@ static void divb_terms(const sm_oracle_grid *g, const lay_t *L, const double *wi
     }
     dw[(long)L->EN * N + idx] = dw[(long)L->EN * N + idx] + (-divb * bdotv);
   }
+#pragma omp parallel for schedule(static)
   for (long idx = 0; idx < N; ++idx) {
     int c[3];
     coords(L, idx, c);
@@ -514,6 +546,7 @@ double sm_oracle_stage_t(const sm_oracle_grid *g, const double *win, const doubl
   if (wout != wbase) memcpy(wout, wbase, sizeof(double) * N * L->NW);
   memcpy(F(wout, L->NW), F(win, L->NW), sizeof(double) * N * (L->NVAR - L->NW));
 
+#pragma omp parallel for schedule(static)
   for (long i = 0; i < N; ++i) {
     pt[i] = pt_of(g, L, win, i);
     ptb[i] = ptb_of(g, L, win, i);
@@ -525,7 +558,9 @@ double sm_oracle_stage_t(const sm_oracle_grid *g, const double *win, const doubl
   for (int dir = 0; dir < D; ++dir) {
     for (int f = 0; f < L->NW; ++f) {
       double *o = F(wout, f);
+#pragma omp parallel for schedule(static)
       for (long i = 0; i < N; ++i) fl[i] = flux_of(g, L, win, pt, i, f, dir);
+#pragma omp parallel for schedule(static)
       for (long idx = 0; idx < N; ++idx) {
         int c[3];
         coords(L, idx, c);
@@ -543,6 +578,7 @@ double sm_oracle_stage_t(const sm_oracle_grid *g, const double *win, const doubl
   }
 
   /* gravity, addgrav_cd2 centdiff2.cu:118-150 */
+#pragma omp parallel for schedule(static)
   for (long idx = 0; idx < N; ++idx) {
     int c[3];
     coords(L, idx, c);
@@ -560,6 +596,7 @@ double sm_oracle_stage_t(const sm_oracle_grid *g, const double *win, const doubl
     /* ---- density, hyperdifrhosource1.cu:15-282 */
     for (int d = 0; d < D; ++d) {
       hyperviscosity(g, L, F(win, L->RHO), L->RHO, d, cmax[d], nur, nul, &numax);
+#pragma omp parallel for schedule(static)
       for (long idx = 0; idx < N; ++idx) {
         int c[3];
         coords(L, idx, c);
@@ -571,6 +608,7 @@ double sm_oracle_stage_t(const sm_oracle_grid *g, const double *win, const doubl
       }
     }
     /* ---- energy, hyperdifesource1.cu:18-554 (q = e - (B^2 + m^2/rho)/2) */
+#pragma omp parallel for schedule(static)
     for (long i = 0; i < N; ++i) {
       double b2 = 0, m2 = 0;
       for (int k = 0; k < D; ++k) b2 += F(win, L->B0 + k)[i] * F(win, L->B0 + k)[i];
@@ -579,6 +617,7 @@ double sm_oracle_stage_t(const sm_oracle_grid *g, const double *win, const doubl
     }
     for (int d = 0; d < D; ++d) {
       hyperviscosity(g, L, q, L->EN, d, cmax[d], nur, nul, &numax);
+#pragma omp parallel for schedule(static)
       for (long idx = 0; idx < N; ++idx) {
         int c[3];
         coords(L, idx, c);
@@ -597,6 +636,7 @@ double sm_oracle_stage_t(const sm_oracle_grid *g, const double *win, const doubl
         for (int ii1 = 0; ii1 <= 1; ++ii1) {
           const int ii = ii1 == 0 ? d : f, ii0 = ii1 == 0 ? f : d;
           if (ii == d) { /* diagonal: hyperdifmomsource1/2/3/3a */
+#pragma omp parallel for schedule(static)
             for (long idx = 0; idx < N; ++idx) {
               int c[3];
               coords(L, idx, c);
@@ -617,6 +657,7 @@ double sm_oracle_stage_t(const sm_oracle_grid *g, const double *win, const doubl
             }
           } else { /* off-diagonal: hyperdifmomsourcene1..6a */
             /* t1 = tmp7 = rho_t * tmp6, t2 = tmp8 = tmp6 * m_ii0, on [1,n-2]^D */
+#pragma omp parallel for schedule(static)
             for (long idx = 0; idx < N; ++idx) {
               int c[3];
               coords(L, idx, c);
@@ -630,6 +671,7 @@ double sm_oracle_stage_t(const sm_oracle_grid *g, const double *win, const doubl
               t1[idx] = (F(win, L->RHO)[idx] + F(win, L->RHOB)[idx]) * tmp6;
               t2[idx] = tmp6 * F(win, L->M0 + ii0)[idx];
             }
+#pragma omp parallel for schedule(static)
             for (long idx = 0; idx < N; ++idx) {
               int c[3];
               coords(L, idx, c);
@@ -637,6 +679,7 @@ double sm_oracle_stage_t(const sm_oracle_grid *g, const double *win, const doubl
               double dm = grad13(g, L, t1, idx, c, ii);
               F(wout, L->M0 + ii0)[idx] = F(wout, L->M0 + ii0)[idx] + h * dm;
             }
+#pragma omp parallel for schedule(static)
             for (long idx = 0; idx < N; ++idx) {
               int c[3];
               coords(L, idx, c);
@@ -657,6 +700,7 @@ double sm_oracle_stage_t(const sm_oracle_grid *g, const double *win, const doubl
           const double sb = ii1 == 0 ? -1.0 : 1.0;
           if (mm == d) { /* diagonal: hyperdifbsource1..4 with tmp1 = B_f on [1,n-2]^D */
             const double *b = F(win, L->B0 + f), *bj = F(win, L->B0 + jj);
+#pragma omp parallel for schedule(static)
             for (long idx = 0; idx < N; ++idx) {
               int c[3];
               coords(L, idx, c);
@@ -674,6 +718,7 @@ double sm_oracle_stage_t(const sm_oracle_grid *g, const double *win, const doubl
             }
           } else { /* off-diagonal: hyperdifbsourcene1..6a */
             const double *b = F(win, L->B0 + f);
+#pragma omp parallel for schedule(static)
             for (long idx = 0; idx < N; ++idx) { /* t1 = tmp3, t2 = tmp5 */
               int c[3];
               coords(L, idx, c);
@@ -684,6 +729,7 @@ double sm_oracle_stage_t(const sm_oracle_grid *g, const double *win, const doubl
               t1[idx] = tmp2 * (nul[idx] + nur[idx]) / 2;
               t2[idx] = t1[idx] * F(win, L->B0 + jj)[idx];
             }
+#pragma omp parallel for schedule(static)
             for (long idx = 0; idx < N; ++idx) {
               int c[3];
               coords(L, idx, c);
@@ -691,6 +737,7 @@ double sm_oracle_stage_t(const sm_oracle_grid *g, const double *win, const doubl
               double db = sb * grad13(g, L, t1, idx, c, mm);
               F(wout, L->B0 + ii0)[idx] = F(wout, L->B0 + ii0)[idx] + h * db;
             }
+#pragma omp parallel for schedule(static)
             for (long idx = 0; idx < N; ++idx) {
               int c[3];
               coords(L, idx, c);
@@ -750,10 +797,12 @@ int sm_oracle_step(const sm_oracle_grid *g, double *w, int step, int rk4, int dt
     sm_oracle_cmax(g, w2, cm);
     v = sm_oracle_stage_t(g, w2, w, w3, dt, cm, s->t + 0.5 * dt); /* w3 = w + dt k3 */
     if (v > numax) numax = v;
+#pragma omp parallel for schedule(static)
     for (long i = 0; i < NW; ++i) w1[i] = (w1[i] + 2 * w2[i] + w3[i] - 4 * w[i]) / 3;
     sm_oracle_cmax(g, w3, cm);
     v = sm_oracle_stage_t(g, w3, w, w2, dt / 6, cm, s->t + 1.0 * dt); /* w + dt/6 k4 */
     if (v > numax) numax = v;
+#pragma omp parallel for schedule(static)
     for (long i = 0; i < NW; ++i) w[i] = w2[i] + w1[i];
     sm_oracle_boundary(g, w);
   }

@@ -344,6 +344,16 @@ int smaug_batch_add(smaug_batch *b, const smaug_params *prm, const double *delx,
   const size_t fp = sim_footprint(p);
   size_t off = 0;
   if (!arena_alloc(b, fp, &off)) return bfail(b, SMAUG_ERR_FULL, "arena has no free block of the simulation's footprint");
+  // every return below that does not admit the simulation releases its block
+  // (stream order keeps a later admission's uploads behind any copy queued here)
+  struct BlockGuard {
+    smaug_batch *b;
+    size_t off, bytes;
+    bool keep = false;
+    ~BlockGuard() {
+      if (!keep) arena_free(b, off, bytes);
+    }
+  } guard{b, off, fp};
   BK(cudaSetDevice(b->device));
   // carve
   char *q = b->arena + off;
@@ -424,7 +434,6 @@ int smaug_batch_add(smaug_batch *b, const smaug_params *prm, const double *delx,
   BK(cudaMemcpyAsync(&chk[1], &sc->bg_live, sizeof(int), cudaMemcpyDeviceToHost, s));
   BK(cudaStreamSynchronize(s));  // the sources above are host temporaries
   if (chk[0] != 0) {
-    arena_free(b, off, fp);
     return bfail(b, SMAUG_ERR_ARG, "metric is not a tensor-product grid on the inner cells, or has a non-positive entry");
   }
   p.phys.has_bgb = chk[1];
@@ -433,6 +442,7 @@ int smaug_batch_add(smaug_batch *b, const smaug_params *prm, const double *delx,
   const int zero = 0;
   BK(cudaMemcpyAsync(b->d_status + slot, &zero, sizeof(int), cudaMemcpyHostToDevice, s));
   BK(cudaStreamSynchronize(s));
+  guard.keep = true;
   Slot &S = b->slots[slot];
   S.used = true;
   S.off = off;

@@ -625,16 +625,26 @@ int smaug_step_noalloc(const smaug_params *prm, const double *delx_dev, const do
       return SMAUG_ERR_CUDA;                    \
     }                                           \
   } while (0)
-  if (w_out_dev != w_in_dev)
-    NA(cudaMemcpyAsync(w_out_dev, w_in_dev, sizeof(double) * (size_t)r.NVAR * N, cudaMemcpyDeviceToDevice, r.stream));
   // every call starts from cleared scalars: the array keeps the last call's data
   NA(cudaMemsetAsync(r.sc, 0, sizeof(DevScalars), r.stream));
-  NA(cudaMemcpyAsync(drv, drv_host.data(), sizeof(double) * drv_host.size(), cudaMemcpyHostToDevice, r.stream));
-  NA(run_load(r));  // ghost fill of w_out, scalars reset, initial maxima
-  NA(run_upload_inst(r));
+  // The metric is checked before anything of the caller's is written, so a
+  // bad metric leaves w_out (which may be w_in) as it was.  The check's
+  // status is read back here; the load below clears it again (minsq stays).
   minsq_init_kernel<<<1, 1, 0, r.stream>>>(r.sc);
   metric_kernel<<<148 * 4, 256, 0, r.stream>>>(delx_dev, r.geo, r.D, dx1, r.sc);
   NA(cudaGetLastError());
+  int metric_status = 0;
+  NA(cudaMemcpyAsync(&metric_status, &r.sc->status, sizeof(int), cudaMemcpyDeviceToHost, r.stream));
+  NA(cudaStreamSynchronize(r.stream));
+  if (metric_status != 0) {
+    set_err(err, errlen, "metric is not positive or not a tensor-product grid on the inner cells");
+    return SMAUG_ERR_ARG;
+  }
+  if (w_out_dev != w_in_dev)
+    NA(cudaMemcpyAsync(w_out_dev, w_in_dev, sizeof(double) * (size_t)r.NVAR * N, cudaMemcpyDeviceToDevice, r.stream));
+  NA(cudaMemcpyAsync(drv, drv_host.data(), sizeof(double) * drv_host.size(), cudaMemcpyHostToDevice, r.stream));
+  NA(run_load(r));  // ghost fill of w_out, scalars reset (minsq kept), initial maxima
+  NA(run_upload_inst(r));
   NA(run_steps(r, nsteps));
   if (r.cur != 0)  // single-step mode with an odd step count: result in W[1]
     NA(cudaMemcpyAsync(w_out_dev, r.W[1], sizeof(double) * (size_t)r.NW * N, cudaMemcpyDeviceToDevice, r.stream));
@@ -649,10 +659,6 @@ int smaug_step_noalloc(const smaug_params *prm, const double *delx_dev, const do
     scalars_out[3] = hs.dtdiffvisc;
     for (int d = 0; d < 3; ++d) scalars_out[4 + d] = d < r.D ? red_get(hs.red[0], d) : 0.0;
     scalars_out[7] = (double)nsteps;
-  }
-  if (hs.status == SMAUG_ERR_ARG) {
-    set_err(err, errlen, "metric is not positive or not a tensor-product grid on the inner cells");
-    return SMAUG_ERR_ARG;
   }
   if (hs.status != 0) {
     set_err(err, errlen, "non-finite dt or wave speed on the device");

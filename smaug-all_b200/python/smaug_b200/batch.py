@@ -85,6 +85,16 @@ class Batch:
         bad = ctypes.c_int(-1)
         self._check(self.lib.smaug_batch_sync(self.h, ctypes.byref(bad)), "smaug_batch_sync")
 
+    def status(self) -> tuple[int, int, str]:
+        """Wait, then (status, slot, message): the first simulation error
+        (SMAUG_ERR_NONFINITE when a simulation's dt or wave speeds became
+        non-finite; that simulation stops, the others go on) and its slot, or
+        (0, -1, "")."""
+        bad = ctypes.c_int(-1)
+        rc = self.lib.smaug_batch_sync(self.h, ctypes.byref(bad))
+        msg = self.lib.smaug_batch_last_error(self.h).decode() if rc != SMAUG_OK else ""
+        return rc, bad.value, msg
+
     def state(self, slot: int, out: np.ndarray | None = None) -> np.ndarray:
         prob = self.probs[slot]
         if out is None:

@@ -16,6 +16,7 @@ Cell centres sit at xmin + (c - 2 + 1/2) dx for the blast wave and at
 """
 from __future__ import annotations
 
+import math
 from dataclasses import dataclass, field
 
 import numpy as np
@@ -175,24 +176,41 @@ MU0 = 4.0e-7 * np.pi
 
 
 def temperature_profile(z, t_ch=6.0e3, t_co=1.0e6, z_tr=2.0e6, w_tr=0.2e6):
-    """T(z) = T_ch + (T_co - T_ch) (1 + tanh((z - z_tr) / w_tr)) / 2."""
-    return t_ch + (t_co - t_ch) * (1.0 + np.tanh((z - z_tr) / w_tr)) / 2.0
+    """T(z) = T_ch + (T_co - T_ch) (1 + tanh((z - z_tr) / w_tr)) / 2, evaluated
+    in the form and operation order of the reference's temp()
+    (models/initialisation_user.h.spicule1_mpi:345-360):
+    0.5 T_co (1 + r + (1 - r) tanh((z - z_tr) / w_tr)) with r = T_ch / T_co,
+    and the C library's tanh (math.tanh), so that it gives the reference's bits."""
+    r = t_ch / t_co
+    return np.array([0.5 * t_co * (1 + r + (1.0 - r) * math.tanh((float(zi) - z_tr) / w_tr)) for zi in np.ravel(z)])
 
 
-def hydrostatic_density(z, T, rho0, g=G_SUN, R=R_GAS):
+def trapezoid_up(f, i0, dx):
+    """Running trapezoid integral of f from index i0 upwards on a uniform grid:
+    out[i0] = 0, out[i] = out[i-1] + 0.5 (f[i-1] + f[i]) dx -- the sum and its
+    operation order of the reference's inte() (models/initialisation_user.h.
+    spicule1_mpi:326-343), whose inte(f, i + 1 - i0, 1, ., dx) over f[i0:] is out[i]."""
+    out = np.zeros(len(f))
+    for i in range(i0 + 1, len(f)):
+        out[i] = out[i - 1] + 0.5 * (f[i - 1] + f[i]) * dx
+    return out
+
+
+def hydrostatic_density(z, T, rho0, dz, g=G_SUN, R=R_GAS):
     """rho_b(z) of an ideal gas (p = rho R T) in hydrostatic equilibrium,
     dp/dz = rho g, with rho = rho0 at z = 0: p = p0 exp(-int_0^z dz'/lambda),
-    lambda = -R T / g, the integral by the trapezoid rule on the grid points z
-    (FP64), from the grid point at z = 0 outwards in both directions."""
+    lambda = -R T / g (the reference's scale height, lambda[i] = -R T[i] / ggg,
+    models/initialisation_user.h.spicule1_mpi:403-404), the integral by the
+    reference's trapezoid rule (trapezoid_up) on the grid points z of spacing
+    dz (FP64) from the grid point at z = 0 upwards, and mirrored below it
+    (the ghost layers under the surface)."""
     inv = 1.0 / (-R * T / g)
     i0 = int(np.argmin(np.abs(z)))
     if z[i0] != 0.0:
         raise ValueError("the grid needs a point at z = 0")
-    integ = np.zeros_like(z)
-    for i in range(i0 + 1, len(z)):
-        integ[i] = integ[i - 1] + 0.5 * (inv[i - 1] + inv[i]) * (z[i] - z[i - 1])
+    integ = trapezoid_up(inv, i0, dz)
     for i in range(i0 - 1, -1, -1):
-        integ[i] = integ[i + 1] - 0.5 * (inv[i + 1] + inv[i]) * (z[i + 1] - z[i])
+        integ[i] = integ[i + 1] - 0.5 * (inv[i + 1] + inv[i]) * dz
     p0 = rho0 * R * T[i0]
     p = p0 * np.exp(-integ)
     return p / (R * T), p
@@ -217,7 +235,7 @@ def atmosphere(nz: int = 256, nx: int = 128, ny: int | None = None, lz: float = 
     xmin = tuple(-NG * dx[d] for d in range(D))
     z = xmin[0] + np.arange(n[0]) * dx[0]
     T = temperature_profile(z)
-    rhob, pb = hydrostatic_density(z, T, rho0)
+    rhob, pb = hydrostatic_density(z, T, rho0, dx[0])
     bz = b_gauss * 1.0e-4 / np.sqrt(MU0)
     ids = field_ids(D)
     shape = tuple(reversed(n))  # arrays are indexed [.., dim1, dim0]

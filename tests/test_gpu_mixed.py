@@ -27,8 +27,9 @@ pytestmark = pytest.mark.gpu
 
 MIXED_RTOL = 1e-5
 # long amplifying runs: mixed drift at most this multiple of the drift of the
-# FP64 FMA build (both measured against the FMA-free FP64 build)
-DRIFT_FACTOR = 10.0
+# FP64 FMA build (both measured against the FMA-free FP64 build); measured
+# 3.7x on the 96^2 Orszag-Tang vortex after 1000 steps (2.1e-2 against 5.7e-3)
+DRIFT_FACTOR = 5.0
 
 
 def field_errors(w, ref, nw):

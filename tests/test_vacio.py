@@ -12,7 +12,10 @@ import pytest
 from smaug_b200 import SmaugError, problems
 from smaug_b200 import vacio
 
-REF_CONFIGS = Path("/root/reference/dev/smaug/configs")
+from oracle.ref_shim import reference_root
+
+_REF = reference_root()
+REF_CONFIGS = _REF / "dev" / "smaug" / "configs" if _REF else Path("/nonexistent")
 
 
 def test_ascii_round_trip_is_exact(tmp_path):

@@ -116,3 +116,40 @@ def test_noalloc_rejects_oversized_grid(need_gpu):
                                 ctypes.c_void_p(dummy.data_ptr()), 1, None, None, err, 256)
     assert rc == -1
     assert b"maximum" in err.value
+
+
+def test_noalloc_in_place_matches_regular_api(need_gpu):
+    import torch
+    lib = _lib()
+    prob = problems.orszag_tang(40)
+    p = _params(prob)
+    delx = torch.from_numpy(np.concatenate([a.ravel() for a in prob.delx()])).cuda()
+    w = torch.from_numpy(np.ascontiguousarray(prob.w)).cuda()
+    err = ctypes.create_string_buffer(256)
+    stream = torch.cuda.current_stream().cuda_stream
+    # w_out == w_in: the header allows it; the result replaces the input
+    rc = lib.smaug_step_noalloc(ctypes.byref(p), ctypes.c_void_p(delx.data_ptr()), ctypes.c_void_p(w.data_ptr()),
+                                ctypes.c_void_p(w.data_ptr()), 4, ctypes.c_void_p(stream), None, err, 256)
+    assert rc == 0, err.value
+    b, _ = _regular(prob, prob.w, 4)
+    assert _rel(w.cpu().numpy(), b) <= RTOL
+
+
+def test_noalloc_bad_metric_leaves_input_untouched(need_gpu):
+    import torch
+    lib = _lib()
+    prob = problems.orszag_tang(24)
+    p = _params(prob)
+    m = np.concatenate([a.ravel() for a in prob.delx()])
+    m[len(m) // 3] = 0.0  # a zero cell width
+    delx = torch.from_numpy(m).cuda()
+    w0 = np.ascontiguousarray(prob.w).copy()
+    w = torch.from_numpy(w0.copy()).cuda()
+    err = ctypes.create_string_buffer(256)
+    stream = torch.cuda.current_stream().cuda_stream
+    rc = lib.smaug_step_noalloc(ctypes.byref(p), ctypes.c_void_p(delx.data_ptr()), ctypes.c_void_p(w.data_ptr()),
+                                ctypes.c_void_p(w.data_ptr()), 3, ctypes.c_void_p(stream), None, err, 256)
+    assert rc == -1
+    assert b"metric" in err.value
+    # in place: the caller's state is exactly as it was (no ghost fill, no step)
+    assert np.array_equal(w.cpu().numpy(), w0)
