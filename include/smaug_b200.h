@@ -159,6 +159,40 @@ int smaug_get_state_device(smaug_ctx *ctx, double *w_dev, size_t count);
 /* Advance nsteps full steps (asynchronous on the context stream). */
 int smaug_step(smaug_ctx *ctx, int nsteps);
 
+/*
+ * The same on the caller's CUDA stream (a cudaStream_t; NULL: the context
+ * stream): the steps wait for all work queued on the context before, and
+ * later context work waits for them, so the caller can order the steps
+ * against its own kernels and copies without a host sync.  Like the
+ * reference's per-step launch sequence (iosmaug.cpp:802-1166), but one call.
+ */
+int smaug_step_on(smaug_ctx *ctx, int nsteps, void *stream);
+
+/*
+ * One Runge-Kutta stage of the current step on the caller's stream (NULL:
+ * the context stream): stages 1..4 in order with rk4 = 1 (stage 1 first
+ * takes the step's dt, stage 4 finishes the step), stage 1 alone with
+ * rk4 = 0.  Calling stages 1..4 is the same work, with the same results, as
+ * smaug_step(ctx, 1); a host loop that interleaves its own work between the
+ * stages uses this.  Out-of-order stages return SMAUG_ERR_STATE, as does
+ * smaug_step while a step begun here is unfinished.  The granularity of the
+ * reference's cuadvance stage slots (advance.cu:18-174) over the fused
+ * operator.
+ */
+int smaug_stage(smaug_ctx *ctx, int stage, void *stream);
+
+/*
+ * The metric from cell positions (host only), replacing initgrid
+ * (init.cu:1118-1670): pos holds ndim arrays of N doubles, the position
+ * components of every cell including ghosts (the reference's wd[pos1..] as
+ * set by init_parallel or read from a VAC file); dx the spacing per dim (it
+ * replaces a zero difference).  delx receives ndim arrays of N doubles for
+ * smaug_set_metric: the positions extrapolated linearly over two layers and a
+ * pad on each side, then centrally differenced, as the reference does.
+ * Errors: SMAUG_ERR_ARG with smaug_vac_last_error().
+ */
+int smaug_initgrid(int ndim, const int *n, const double *pos, const double *dx, double *delx);
+
 /* Wait for all queued work; returns the first device-side error if any. */
 int smaug_sync(smaug_ctx *ctx);
 

@@ -194,51 +194,59 @@ cudaError_t run_combine(Run &r) {
   return cudaGetLastError();
 }
 
-// Enqueue nsteps full steps.
-cudaError_t run_steps(Run &r, int nsteps) {
-  for (int it = 0; it < nsteps; ++it) {
+// Stages per step: four for RK4, one for the single step.
+inline int stages_per_step(const Run &r) { return r.rk4 ? 4 : 1; }
+
+// Enqueue stage k (1..stages_per_step) of a step: stage 1 opens the step with
+// the dt kernel, the last stage closes it with the finish kernel.
+cudaError_t run_stage(Run &r, int k) {
+  if (k == 1) {
     dt_kernel<<<1, 1, 0, r.stream>>>(r.sc, r.phys, r.D);
     r.launches++;
-    StageArgs a{};
-    a.bg = r.bg;
-    a.sc = r.sc;
-    if (r.mixed) {
-      // the same fourstep with FP32 stage states: S1 = W + dt/2 L(W),
-      // S2 = W + dt/2 L(S1), S3 = W + dt L(S2), A = (S1 + 2 S2 + S3 - 4 W)/3
-      // accumulated stage by stage, W <- W + dt/6 L(S3) + A (stage roles in
-      // batch_args, batch_kernels.cu)
-      for (int k = 1; k <= 4; ++k) launch_rk_stage(r, k);
-      finish_kernel<<<1, 1, 0, r.stream>>>(r.sc, 4);
-    } else if (!r.rk4) {
-      double *w = r.W[r.cur], *o = r.W[1 - r.cur];
-      a.in = w; a.base = w; a.out = o; a.acc = nullptr; a.kind = 0;
-      a.red_in = 0; a.red_out = 1; a.hdiv = 1.0; a.tfrac = 0.0;
-      launch_stage(r, a);
-      finish_kernel<<<1, 1, 0, r.stream>>>(r.sc, 1);
-      r.cur = 1 - r.cur;
-    } else if (!r.exact) {
-      // production FP64 fourstep: the same stage roles in the batch kernel
-      for (int k = 1; k <= 4; ++k) launch_rk_stage(r, k);
-      finish_kernel<<<1, 1, 0, r.stream>>>(r.sc, 4);
-    } else {
-      // SAC fourstep (vac.t:447-462): W1 = W + dt/2 L(W); W2 = W + dt/2 L(W1);
-      // W3 = W + dt L(W2) and W1 <- (W1 + 2 W2 + W3 - 4 W)/3; W <- (W + dt/6 L(W3)) + W1
-      double *W = r.W[0], *W1 = r.W[1], *W2 = r.W[2], *W3 = r.W[3];
-      a.base = W;
-      a.in = W;  a.out = W1; a.acc = nullptr; a.kind = 0; a.red_in = 0; a.red_out = 1; a.hdiv = 2.0; a.tfrac = 0.0;
-      launch_stage(r, a);
-      a.in = W1; a.out = W2; a.red_in = 1; a.red_out = 2; a.hdiv = 2.0; a.tfrac = 0.5;
-      launch_stage(r, a);
-      a.in = W2; a.out = W3; a.acc = W1; a.kind = 3; a.red_in = 2; a.red_out = 3; a.hdiv = 1.0; a.tfrac = 0.5;
-      launch_stage(r, a);
-      a.in = W3; a.out = W;  a.acc = W1; a.kind = 4; a.red_in = 3; a.red_out = 4; a.hdiv = 6.0; a.tfrac = 1.0;
-      launch_stage(r, a);
-      finish_kernel<<<1, 1, 0, r.stream>>>(r.sc, 4);
-    }
-    r.launches++;
-    cudaError_t e = cudaGetLastError();
-    if (e != cudaSuccess) return e;
   }
+  StageArgs a{};
+  a.bg = r.bg;
+  a.sc = r.sc;
+  if (r.mixed || (r.rk4 && !r.exact)) {
+    // production fourstep, FP64 or mixed (FP32 stage states: S1 = W + dt/2
+    // L(W), S2 = W + dt/2 L(S1), S3 = W + dt L(S2), A = (S1 + 2 S2 + S3 -
+    // 4 W)/3 accumulated stage by stage, W <- W + dt/6 L(S3) + A); the stage
+    // roles are in batch_args (batch_kernels.inc)
+    launch_rk_stage(r, k);
+  } else if (!r.rk4) {
+    double *w = r.W[r.cur], *o = r.W[1 - r.cur];
+    a.in = w; a.base = w; a.out = o; a.acc = nullptr; a.kind = 0;
+    a.red_in = 0; a.red_out = 1; a.hdiv = 1.0; a.tfrac = 0.0;
+    launch_stage(r, a);
+    r.cur = 1 - r.cur;
+  } else {
+    // SAC fourstep (vac.t:447-462): W1 = W + dt/2 L(W); W2 = W + dt/2 L(W1);
+    // W3 = W + dt L(W2) and W1 <- (W1 + 2 W2 + W3 - 4 W)/3; W <- (W + dt/6 L(W3)) + W1
+    double *W = r.W[0], *W1 = r.W[1], *W2 = r.W[2], *W3 = r.W[3];
+    a.base = W;
+    switch (k) {
+      case 1: a.in = W;  a.out = W1; a.acc = nullptr; a.kind = 0; a.red_in = 0; a.red_out = 1; a.hdiv = 2.0; a.tfrac = 0.0; break;
+      case 2: a.in = W1; a.out = W2; a.acc = nullptr; a.kind = 0; a.red_in = 1; a.red_out = 2; a.hdiv = 2.0; a.tfrac = 0.5; break;
+      case 3: a.in = W2; a.out = W3; a.acc = W1; a.kind = 3; a.red_in = 2; a.red_out = 3; a.hdiv = 1.0; a.tfrac = 0.5; break;
+      default: a.in = W3; a.out = W; a.acc = W1; a.kind = 4; a.red_in = 3; a.red_out = 4; a.hdiv = 6.0; a.tfrac = 1.0; break;
+    }
+    launch_stage(r, a);
+  }
+  if (k == stages_per_step(r)) {
+    finish_kernel<<<1, 1, 0, r.stream>>>(r.sc, k);
+    r.launches++;
+  }
+  return cudaGetLastError();
+}
+
+// Enqueue nsteps full steps.
+cudaError_t run_steps(Run &r, int nsteps) {
+  const int ns = stages_per_step(r);
+  for (int it = 0; it < nsteps; ++it)
+    for (int k = 1; k <= ns; ++k) {
+      const cudaError_t e = run_stage(r, k);
+      if (e != cudaSuccess) return e;
+    }
   return cudaSuccess;
 }
 
@@ -257,6 +265,8 @@ struct smaug_ctx {
   bool profile = false;
   std::vector<cudaEvent_t> ev;
   size_t ev_used = 0;
+  int next_stage = 1;          // smaug_stage: the stage the current step takes next
+  cudaEvent_t join = nullptr;  // orders the context stream and a caller's stream
 };
 
 namespace {
@@ -313,6 +323,7 @@ int smaug_create(const smaug_params *prm, int device, smaug_ctx **out) {
     }
   }
   CK(cudaMemsetAsync(r.sc, 0, sizeof(DevScalars), r.stream));
+  CK(cudaEventCreateWithFlags(&ctx->join, cudaEventDisableTiming));
   CK(cudaStreamSynchronize(r.stream));
   return SMAUG_OK;
 }
@@ -332,6 +343,7 @@ int smaug_destroy(smaug_ctx *ctx) {
   cudaFree(r.inst);
   drop_graphs(r);
   for (auto e : ctx->ev) cudaEventDestroy(e);
+  if (ctx->join) cudaEventDestroy(ctx->join);
   if (r.stream) cudaStreamDestroy(r.stream);
   delete ctx;
   return SMAUG_OK;
@@ -394,6 +406,7 @@ static int load_state(smaug_ctx *ctx, const double *w, size_t count, cudaMemcpyK
   // the graphs hold the physics by value (dt kernel): recapture if it changed
   if (memcmp(&before, &r.phys, sizeof(Phys)) != 0) drop_graphs(r);
   ctx->steps = 0;
+  ctx->next_stage = 1;
   return SMAUG_OK;
 }
 
@@ -428,7 +441,7 @@ int smaug_get_state_device(smaug_ctx *ctx, double *w, size_t count) {
 // The steps of the production RK4 path as graph replays: the launch sequence
 // of a step is the same every step (the batch stage kernel over this
 // simulation's one-entry table, its ghost pass, the dt and finish kernels).
-cudaError_t run_steps_graphed(Run &r, int nsteps) {
+cudaError_t ensure_graphs(Run &r) {
   const int len[2] = {kGraphSteps, 1};
   for (int k = 0; k < 2; ++k) {
     if (r.graph[k]) continue;
@@ -446,6 +459,12 @@ cudaError_t run_steps_graphed(Run &r, int nsteps) {
     cudaGraphDestroy(g);
     if (e != cudaSuccess) return e;
   }
+  return cudaSuccess;
+}
+
+cudaError_t run_steps_graphed(Run &r, int nsteps) {
+  const cudaError_t eg = ensure_graphs(r);
+  if (eg != cudaSuccess) return eg;
   for (; nsteps >= kGraphSteps; nsteps -= kGraphSteps) {
     const cudaError_t e = cudaGraphLaunch(r.graph[0], r.stream);
     if (e != cudaSuccess) return e;
@@ -459,10 +478,7 @@ cudaError_t run_steps_graphed(Run &r, int nsteps) {
   return cudaSuccess;
 }
 
-int smaug_step(smaug_ctx *ctx, int nsteps) {
-  if (!ctx || nsteps < 0) return SMAUG_ERR_ARG;
-  if (!ctx->have_state) return fail(ctx, SMAUG_ERR_STATE, "no state loaded");
-  CK(cudaSetDevice(ctx->device));
+static int step_impl(smaug_ctx *ctx, int nsteps) {
   Run &r = ctx->run;
   r.ev_used = ctx->profile ? &ctx->ev_used : nullptr;
   if (r.rk4 && !r.exact && !ctx->profile)
@@ -470,6 +486,63 @@ int smaug_step(smaug_ctx *ctx, int nsteps) {
   else
     CK(run_steps(r, nsteps));
   ctx->steps += nsteps;
+  return SMAUG_OK;
+}
+
+int smaug_step(smaug_ctx *ctx, int nsteps) {
+  if (!ctx || nsteps < 0) return SMAUG_ERR_ARG;
+  if (!ctx->have_state) return fail(ctx, SMAUG_ERR_STATE, "no state loaded");
+  if (ctx->next_stage != 1) return fail(ctx, SMAUG_ERR_STATE, "a step begun by smaug_stage is not finished");
+  CK(cudaSetDevice(ctx->device));
+  return step_impl(ctx, nsteps);
+}
+
+// Run `body` with the context's launches on the caller's stream s: s first
+// waits for everything queued on the context stream, and the context stream
+// then waits for s, so work queued on either later stays in order.
+extern "C++" {
+template <typename F>
+int on_stream(smaug_ctx *ctx, cudaStream_t s, F body) {
+  Run &r = ctx->run;
+  const cudaStream_t own = r.stream;
+  if (!s || s == own) return body();
+  CK(cudaEventRecord(ctx->join, own));
+  CK(cudaStreamWaitEvent(s, ctx->join, 0));
+  r.stream = s;
+  const int rc = body();
+  r.stream = own;
+  CK(cudaEventRecord(ctx->join, s));
+  CK(cudaStreamWaitEvent(own, ctx->join, 0));
+  return rc;
+}
+}  // extern "C++"
+
+int smaug_step_on(smaug_ctx *ctx, int nsteps, void *stream) {
+  if (!ctx || nsteps < 0) return SMAUG_ERR_ARG;
+  if (!ctx->have_state) return fail(ctx, SMAUG_ERR_STATE, "no state loaded");
+  if (ctx->next_stage != 1) return fail(ctx, SMAUG_ERR_STATE, "a step begun by smaug_stage is not finished");
+  CK(cudaSetDevice(ctx->device));
+  // the graphs are captured on the context's own stream, never the caller's
+  if (ctx->run.rk4 && !ctx->run.exact && !ctx->profile) CK(ensure_graphs(ctx->run));
+  return on_stream(ctx, (cudaStream_t)stream, [&] { return step_impl(ctx, nsteps); });
+}
+
+int smaug_stage(smaug_ctx *ctx, int stage, void *stream) {
+  if (!ctx) return SMAUG_ERR_ARG;
+  if (!ctx->have_state) return fail(ctx, SMAUG_ERR_STATE, "no state loaded");
+  Run &r = ctx->run;
+  const int ns = stages_per_step(r);
+  if (stage < 1 || stage > ns) return fail(ctx, SMAUG_ERR_ARG, "stage must be 1..4 (RK4) or 1 (single step)");
+  if (stage != ctx->next_stage) return fail(ctx, SMAUG_ERR_STATE, "stages of a step must come in order 1, 2, ...");
+  CK(cudaSetDevice(ctx->device));
+  r.ev_used = ctx->profile ? &ctx->ev_used : nullptr;
+  const int rc = on_stream(ctx, (cudaStream_t)stream, [&]() -> int {
+    CK(run_stage(r, stage));
+    return SMAUG_OK;
+  });
+  if (rc != SMAUG_OK) return rc;
+  ctx->next_stage = stage == ns ? 1 : stage + 1;
+  if (stage == ns) ctx->steps += 1;
   return SMAUG_OK;
 }
 

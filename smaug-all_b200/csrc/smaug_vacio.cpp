@@ -241,3 +241,68 @@ int smaug_vac_read_binary(const char *path, smaug_vac_header *hdr, double *pos, 
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// smaug_initgrid: the metric from cell positions, as the reference's initgrid
+// (init.cu:1118-1670) derives it from wd[pos1..] (the positions of every cell,
+// ghosts included, as init_parallel sets them or a VAC file holds them):
+//   * the positions go into a copy padded by one layer on each side of every
+//     dimension (2-D: x and y only);
+//   * dimension by dimension, every position component is extrapolated
+//     linearly over the two outermost layers and the pad of each side,
+//     q(ix) = (1 + |ixe - ix|) q(ixe) - |ixe - ix| q(ixf) with ixe, ixf the
+//     first two inner cells of that side;
+//   * delx_d = (x_d[c + 1] - x_d[c - 1]) / 2 along d, where 0 becomes dx[d].
+// Built without FMA contraction (the build passes -ffp-contract=off), so the
+// metric has the reference's bits.
+// ---------------------------------------------------------------------------
+extern "C" int smaug_initgrid(int ndim, const int *n, const double *pos, const double *dx, double *delx) {
+  if (ndim != 2 && ndim != 3) return vfail("ndim must be 2 or 3");
+  if (!n || !pos || !dx || !delx) return vfail("null argument");
+  const int D = ndim;
+  int nn[3] = {n[0], n[1], D == 3 ? n[2] : 1};
+  for (int d = 0; d < D; ++d)
+    if (nn[d] < 5 || nn[d] > (1 << 20)) return vfail("each dimension needs 5..2^20 cells including ghosts");
+  const long long N = (long long)nn[0] * nn[1] * nn[2];
+  const int pn[3] = {nn[0] + 2, nn[1] + 2, D == 3 ? nn[2] + 2 : 1};
+  const size_t Np = (size_t)pn[0] * pn[1] * pn[2];
+  const size_t ps[3] = {1, (size_t)pn[0], (size_t)pn[0] * pn[1]};
+  const int off3 = D == 3 ? 1 : 0;
+  std::vector<std::vector<double>> T(D, std::vector<double>(Np, 0.0));
+  for (int d1 = 0; d1 < D; ++d1) {
+    const double *src = pos + (size_t)d1 * N;
+    for (int k = 0; k < nn[2]; ++k)
+      for (int j = 0; j < nn[1]; ++j)
+        for (int i = 0; i < nn[0]; ++i)
+          T[d1][(size_t)(i + 1) + ps[1] * (j + 1) + ps[2] * (k + off3)] = src[i + (size_t)nn[0] * (j + (size_t)nn[1] * k)];
+  }
+  for (int d = 0; d < D; ++d) {
+    const int m = nn[d];
+    // the other two axes of the padded copy (full padded ranges)
+    const int a1 = d == 0 ? 1 : 0, a2 = d == 2 ? 1 : 2;
+    const int sides[2][4] = {{m - 1, m + 1, m - 2, m - 3}, {0, 2, 3, 4}};
+    for (const auto &sd : sides)
+      for (int d1 = 0; d1 < D; ++d1)
+        for (int ix = sd[0]; ix <= sd[1]; ++ix) {
+          const double a = (double)std::abs(sd[2] - ix);
+          for (int u = 0; u < pn[a2]; ++u)
+            for (int v = 0; v < pn[a1]; ++v) {
+              const size_t base = ps[a1] * v + ps[a2] * u;
+              double *t = T[d1].data();
+              t[base + ps[d] * ix] = (1.0 + a) * t[base + ps[d] * sd[2]] - a * t[base + ps[d] * sd[3]];
+            }
+        }
+  }
+  for (int d = 0; d < D; ++d) {
+    const double *t = T[d].data();
+    double *out = delx + (size_t)d * N;
+    for (int k = 0; k < nn[2]; ++k)
+      for (int j = 0; j < nn[1]; ++j)
+        for (int i = 0; i < nn[0]; ++i) {
+          const size_t c = (size_t)(i + 1) + ps[1] * (j + 1) + ps[2] * (k + off3);
+          const double v = 0.5 * (t[c + ps[d]] - t[c - ps[d]]);
+          out[i + (size_t)nn[0] * (j + (size_t)nn[1] * k)] = v == 0.0 ? dx[d] : v;
+        }
+  }
+  return SMAUG_OK;
+}

@@ -61,6 +61,10 @@ def load_library(path: Path | None = None):
     L.smaug_set_state_device.argtypes = [ctypes.c_void_p, ctypes.c_void_p, _SZ]
     L.smaug_get_state_device.argtypes = [ctypes.c_void_p, ctypes.c_void_p, _SZ]
     L.smaug_step.argtypes = [ctypes.c_void_p, _I]
+    L.smaug_step_on.argtypes = [ctypes.c_void_p, _I, ctypes.c_void_p]
+    L.smaug_stage.argtypes = [ctypes.c_void_p, _I, ctypes.c_void_p]
+    L.smaug_initgrid.argtypes = [_I, ctypes.POINTER(_I), _PD, _PD, _PD]
+    L.smaug_vac_last_error.restype = ctypes.c_char_p
     L.smaug_sync.argtypes = [ctypes.c_void_p]
     L.smaug_get_scalars.argtypes = [ctypes.c_void_p, _PD]
     L.smaug_stream.argtypes = [ctypes.c_void_p]
@@ -101,6 +105,22 @@ def load_library(path: Path | None = None):
 
 def _f64(a) -> np.ndarray:
     return np.ascontiguousarray(a, dtype=np.float64)
+
+
+def initgrid(n, pos, dx) -> list:
+    """The metric from cell positions (smaug_initgrid, the reference's
+    initgrid): pos is ndim grid-shaped arrays (storage order [k,] j, i) of the
+    position components of every cell; returns ndim grid-shaped arrays."""
+    lib = load_library()
+    D = len(n)
+    pos = _f64(np.stack([np.asarray(p) for p in pos]))
+    out = np.empty_like(pos)
+    nn = (_I * 3)(*(list(n) + [1] * (3 - D)))
+    d = (_D * 3)(*(list(dx) + [0.0] * (3 - D)))
+    rc = lib.smaug_initgrid(D, nn, pos.ctypes.data_as(_PD), d, out.ctypes.data_as(_PD))
+    if rc != SMAUG_OK:
+        raise SmaugError(f"smaug_initgrid failed ({rc}): {lib.smaug_vac_last_error().decode()}")
+    return [out[k] for k in range(D)]
 
 
 def make_params(prob, rk4: bool = True, dt_mode: int = 1, exact: bool = False, dt0: float = 0.0,
@@ -180,6 +200,14 @@ class Engine:
 
     def step(self, n: int = 1):
         self._check(self.lib.smaug_step(self.h, n), "smaug_step")
+
+    def step_on(self, n: int, stream: int):
+        """n steps on the caller's CUDA stream (a cudaStream_t handle)."""
+        self._check(self.lib.smaug_step_on(self.h, n, ctypes.c_void_p(stream)), "smaug_step_on")
+
+    def stage(self, k: int, stream: int = 0):
+        """RK stage k (1..4; 1 in single-step mode) of the current step."""
+        self._check(self.lib.smaug_stage(self.h, k, ctypes.c_void_p(stream)), "smaug_stage")
 
     def sync(self):
         self._check(self.lib.smaug_sync(self.h), "smaug_sync")

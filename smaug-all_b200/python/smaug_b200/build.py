@@ -33,19 +33,36 @@ UNITS = [
     ("batch_k3d.cu", ["-fmad=true", "-ftz=true"]),
     ("smaug_capi.cu", []),
     ("smaug_batch.cu", []),
-    ("smaug_vacio.cpp", []),
+    ("smaug_vacio.cpp", ["-Xcompiler", "-ffp-contract=off"]),
 ]
+
+
+HOST_DRIVER = PKG / "host" / "smaug_run.c"
+HOST_EXE = LIBDIR / "smaug_run"
+
+
+def build_host_driver() -> Path:
+    """The C host driver (host/smaug_run.c), linked against the library; it
+    sits beside the library and finds it through its run path."""
+    cuda = Path(os.environ.get("CUDA_HOME", "/usr/local/cuda"))
+    cmd = ["gcc", "-O2", "-std=c99", "-Wall", "-I", str(PKG.parent / "include"), "-I", str(cuda / "include"),
+           str(HOST_DRIVER), "-L", str(LIBDIR), "-lsmaug_b200", "-L", str(cuda / "lib64"), "-lcudart",
+           "-Wl,-rpath,$ORIGIN", "-o", str(HOST_EXE)]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"host driver build failed:\n{' '.join(cmd)}\n{r.stderr[-4000:]}")
+    return HOST_EXE
 
 
 def sources():
     # this file too: its flags are part of what the library is built from
     return sorted(CSRC.glob("*.cu")) + sorted(CSRC.glob("*.cpp")) + sorted(CSRC.glob("*.cuh")) + sorted(
         CSRC.glob("*.inc")) + [
-        PKG.parent / "include" / "smaug_b200.h", Path(__file__).resolve()]
+        PKG.parent / "include" / "smaug_b200.h", Path(__file__).resolve(), HOST_DRIVER]
 
 
 def up_to_date() -> bool:
-    if not LIB.exists():
+    if not LIB.exists() or not HOST_EXE.exists():
         return False
     t = LIB.stat().st_mtime
     return all(s.stat().st_mtime <= t for s in sources())
@@ -78,6 +95,7 @@ def build(force: bool = False, verbose: bool = False) -> Path:
     if r.returncode != 0:
         raise RuntimeError(f"link failed:\n{r.stderr[-4000:]}")
     os.replace(tmp, LIB)
+    build_host_driver()
     return LIB
 
 

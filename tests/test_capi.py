@@ -6,6 +6,7 @@ import ctypes
 import re
 from pathlib import Path
 
+import numpy as np
 import pytest
 
 from smaug_b200 import LIB_PATH, load_library
@@ -120,3 +121,36 @@ def test_params_struct_layout_matches_header(tmp_path):
     vals = [int(x) for x in subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split()]
     assert vals[0] == ctypes.sizeof(Params)
     assert vals[1:] == [getattr(Params, n).offset for n in names]
+
+
+def test_initgrid_bits_equal_reference_metric():
+    """smaug_initgrid (C++, the reference's initgrid from positions) gives the
+    bits of problems.metric, the restatement the oracle and the fixtures use,
+    on 2-D and 3-D grids with positions as init_parallel sets them."""
+    from smaug_b200 import initgrid, problems
+    for prob in (problems.orszag_tang(20, ny=12), problems.blast_wave(7, seed=2), problems.atmosphere(24, 10)):
+        D = prob.ndim
+        shape = prob.w.shape[1:]
+        pos = []
+        for d in range(D):
+            x = prob.xmin[d] + np.arange(prob.n[d]) * prob.dx[d]
+            view = [1] * D
+            view[D - 1 - d] = prob.n[d]
+            pos.append(np.broadcast_to(x.reshape(view), shape))
+        got = initgrid(prob.n, pos, prob.dx)
+        want = prob.delx()
+        for d in range(D):
+            assert np.array_equal(got[d], want[d]), (prob.name, d)
+
+
+def test_host_driver_is_built_and_links():
+    """The C host driver links against the library and runs without a GPU
+    as far as its usage text."""
+    import subprocess
+
+    from smaug_b200.build import HOST_EXE
+    assert HOST_EXE.exists(), "smaug_run not built"
+    r = subprocess.run([str(HOST_EXE), "--help"], capture_output=True, text=True)
+    assert r.returncode == 0 and "usage: smaug_run" in r.stderr
+    r = subprocess.run([str(HOST_EXE)], capture_output=True, text=True)
+    assert r.returncode == 2
