@@ -58,14 +58,51 @@ def sources():
     # this file too: its flags are part of what the library is built from
     return sorted(CSRC.glob("*.cu")) + sorted(CSRC.glob("*.cpp")) + sorted(CSRC.glob("*.cuh")) + sorted(
         CSRC.glob("*.inc")) + [
-        PKG.parent / "include" / "smaug_b200.h", Path(__file__).resolve(), HOST_DRIVER]
+        PKG.parent / "include" / "smaug_b200.h", PKG.parent / "include" / "smaug_cukernels.h",
+        Path(__file__).resolve(), HOST_DRIVER, REF_LOOP]
 
 
 def up_to_date() -> bool:
-    if not LIB.exists() or not HOST_EXE.exists():
+    if not LIB.exists() or not HOST_EXE.exists() or not all((LIBDIR / e).exists() for _, _, e in COMPAT):
         return False
     t = LIB.stat().st_mtime
     return all(s.stat().st_mtime <= t for s in sources())
+
+
+# The reference-compatible per-operator entry points (include/smaug_cukernels.h),
+# one library per dimensionality, built without FMA contraction, and the
+# reference-shaped host loop over each (host/ref_loop.c).
+COMPAT = [(2, "libsmaug_cu2d.so", "smaug_ref_loop2d"), (3, "libsmaug_cu3d.so", "smaug_ref_loop3d")]
+REF_LOOP = PKG / "host" / "ref_loop.c"
+
+
+def compat_lib(ndim: int) -> Path:
+    return LIBDIR / dict((d, lib) for d, lib, _ in COMPAT)[ndim]
+
+
+def ref_loop_exe(ndim: int) -> Path:
+    return LIBDIR / dict((d, exe) for d, _, exe in COMPAT)[ndim]
+
+
+def build_compat(objdir: Path) -> None:
+    def one(entry):
+        D, lib, exe = entry
+        obj = objdir / f"smaug_cucompat{D}d.o"
+        cmd = [NVCC, *COMMON, "-fmad=false", f"-DSMAUG_CU_NDIM={D}", "-c", str(CSRC / "smaug_cucompat.cu"),
+               "-o", str(obj)]
+        steps = [cmd,
+                 [NVCC, "-shared", *ARCH, "-o", str(LIBDIR / lib), str(obj), "-L", str(LIBDIR), "-lsmaug_b200",
+                  "-lcudart", "-Xlinker", "-rpath=$ORIGIN"],
+                 ["gcc", "-O2", "-std=c99", "-Wall", f"-DSMAUG_CU_NDIM={D}", "-I", str(PKG.parent / "include"),
+                  str(REF_LOOP), "-L", str(LIBDIR), f"-l:{lib}", "-lsmaug_b200", "-Wl,-rpath,$ORIGIN", "-o",
+                  str(LIBDIR / exe)]]
+        for c in steps:
+            r = subprocess.run(c, capture_output=True, text=True)
+            if r.returncode != 0:
+                raise RuntimeError(f"compat build failed:\n{' '.join(c)}\n{r.stderr[-6000:]}")
+
+    with ThreadPoolExecutor(max_workers=len(COMPAT)) as ex:
+        list(ex.map(one, COMPAT))
 
 
 def build(force: bool = False, verbose: bool = False) -> Path:
@@ -96,6 +133,7 @@ def build(force: bool = False, verbose: bool = False) -> Path:
         raise RuntimeError(f"link failed:\n{r.stderr[-4000:]}")
     os.replace(tmp, LIB)
     build_host_driver()
+    build_compat(objdir)
     return LIB
 
 
