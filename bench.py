@@ -58,7 +58,6 @@ BYTES_PER_CELL_UPDATE_MIXED_3D = alg_bytes_per_cell_update(3, True)   # 608 B
 # in all: 2-D 584 B, 3-D 768 B.
 DESIGN_BYTES_MIXED = {2: 19 * 6 * 4 + 4 * 4 * 8, 3: 19 * 8 * 4 + 4 * 5 * 8}
 ENSEMBLE = {"count": 96, "seed": 4242}
-SAMPLE_N = 128         # CPU sample: one 128^2 Orszag-Tang simulation of the ensemble per process
 SAMPLE_SUBSTEPS = 4    # reference single steps per RK4-equivalent step
 
 
@@ -84,66 +83,118 @@ def load_traffic():
 # ----------------------------------------------------------------- CPU side
 
 def _cpu_worker(args):
-    n, substeps, nsteps, warmup, use_ref, rank = args
-    # the reference's host code prints progress on stdout; keep the bench's
-    # stdout to its one JSON line
+    """One simulation on one host core: (side, RK4-equivalent steps, timed
+    seconds).  The reference's host code prints progress on stdout; it is sent
+    to /dev/null so the bench's stdout keeps its one JSON line."""
+    prob_args, substeps, min_steps, budget_s, use_ref = args
     devnull = os.open(os.devnull, os.O_WRONLY)
     os.dup2(devnull, 1)
     from smaug_b200 import problems
-    cfg = ENSEMBLE
-    prob = problems.orszag_tang(n, b0_scale=1.0, rho_noise=0.01, seed=cfg["seed"] + rank)
+    prob = problems.orszag_tang(**prob_args)
     if use_ref:
         from oracle.oracle import Reference
         sim = Reference(prob)
-        sim.step(warmup * substeps)
-        t = time.perf_counter()
-        for _ in range(nsteps):
-            sim.step(substeps)
+        sim.step(1)  # warm-up: one reference single step
+        adv = lambda: sim.step(substeps)  # noqa: E731
     else:
         from oracle.oracle import Oracle
         sim = Oracle(prob)
-        sim.step(warmup, rk4=True)
-        t = time.perf_counter()
-        sim.step(nsteps, rk4=True)
-    return time.perf_counter() - t
+        sim.step(1, rk4=True)
+        adv = lambda: sim.step(1, rk4=True)  # noqa: E731
+    steps, t = 0, time.perf_counter()
+    while steps < min_steps or (time.perf_counter() - t < budget_s and steps < 64):
+        adv()
+        steps += 1
+    return prob_args["nx"], steps, time.perf_counter() - t
 
 
-def cpu_throughput(nsteps: int, warmup: int = 1, procs: int | None = None):
-    """Cell-updates/s of the reference's CPU code on the host cores."""
+def _cpu_pool(jobs, procs):
     import multiprocessing as mp
-    use_ref = (ROOT / "oracle" / "_ref" / "libsmaug_ref2d.so").exists()
+    with mp.get_context("spawn").Pool(procs) as pool:
+        return pool.map(_cpu_worker, jobs, chunksize=1)
+
+
+def _use_ref() -> bool:
+    return (ROOT / "oracle" / "_ref" / "libsmaug_ref2d.so").exists()
+
+
+def cpu_throughput(procs: int | None = None, budget_s: float = 4.0):
+    """Cell-updates/s of the reference's CPU code on the ensemble workload,
+    from a bounded sample: one member of each side of the ensemble (128 ..
+    768) advanced for at least one RK4-equivalent step (4 reference single
+    steps; the reference's rkon=1 path is not usable) and for about
+    `budget_s` seconds, one simulation per host process.  The per-side rates
+    are combined with the 96-member ensemble's own mix of sides: time per
+    ensemble step = sum over members of cells / rate(side), run on `procs`
+    cores, so value = procs * cells / that time."""
+    from smaug_b200 import problems
+    use_ref = _use_ref()
     procs = procs or os.cpu_count() or 1
-    ctx = mp.get_context("spawn")
     substeps = SAMPLE_SUBSTEPS if use_ref else 1
+    ens = problems.ensemble(ENSEMBLE["count"], seed=ENSEMBLE["seed"])
+    sample = {}
+    for i, p in enumerate(ens):  # the first member of each side
+        side = p.n[0] - 4
+        if side not in sample:
+            m = p.meta
+            sample[side] = dict(nx=side, b0_scale=m["b0_scale"], rho_noise=m["rho_noise"], seed=m["seed"])
+    jobs = [(sample[s], substeps, 1, budget_s, use_ref) for s in sorted(sample, reverse=True)]
     t0 = time.perf_counter()
-    with ctx.Pool(procs) as pool:
-        times = pool.map(_cpu_worker, [(SAMPLE_N, substeps, nsteps, warmup, use_ref, r) for r in range(procs)])
+    res = _cpu_pool(jobs, min(procs, len(jobs)))
     wall = time.perf_counter() - t0
-    elapsed = max(times)
-    cells = SAMPLE_N ** 2
-    value = procs * cells * nsteps / elapsed
+    rate = {side: side * side * steps / sec for side, steps, sec in res}  # cell-updates/s on one core
+    cells = [p.interior for p in ens]
+    t_one_core = sum(c / rate[int(round(c ** 0.5))] for c in cells)
+    value = procs * sum(cells) / t_one_core
     kind = "reference" if use_ref else "port"
-    sample = (f"{procs} processes x one {SAMPLE_N}^2 Orszag-Tang simulation of the ensemble x {nsteps} "
-              "RK4-equivalent steps " + (f"({substeps} reference single steps each; the reference's rkon=1 path "
-                                         "is not usable)" if use_ref else "(oracle port, RK4)"))
-    return {"value": value, "unit": UNIT, "cores": procs, "kind": kind, "sample": sample,
-            "elapsed_s": elapsed, "wall_s": wall}
+    desc = (f"one ensemble member of each side ({', '.join(str(s) for s in sorted(sample))}) for >= 1 RK4-equivalent "
+            f"step and ~{budget_s:.0f} s each, one process per member"
+            + (f" ({substeps} reference single steps per RK4-equivalent step; the reference's rkon=1 path is not "
+               "usable)" if use_ref else " (oracle port, RK4)")
+            + f"; per-side rates weighted by the 96-member mix, scaled to {procs} cores")
+    return {"value": value, "unit": UNIT, "cores": procs, "kind": kind, "sample": desc,
+            "per_side_rate_one_core": {str(k): v for k, v in sorted(rate.items())}, "wall_s": wall}
+
+
+def cpu_c1(nsteps: int = 2):
+    """configs[0] on the host: Orszag-Tang 256^2 through the reference's CPU
+    build, `nsteps` RK4-equivalent steps, on 1 process and on nproc processes
+    (one independent copy of the simulation per core: the reference's host
+    build is single-threaded)."""
+    use_ref = _use_ref()
+    substeps = SAMPLE_SUBSTEPS if use_ref else 1
+    args = dict(nx=256)
+    nproc = os.cpu_count() or 1
+    one = _cpu_pool([(args, substeps, nsteps, 0.0, use_ref)], 1)[0]
+    many = _cpu_pool([(args, substeps, nsteps, 0.0, use_ref)] * nproc, nproc)
+    cells = 256 * 256
+    v1 = cells * one[1] / one[2]
+    vn = sum(cells * r[1] for r in many) / max(r[2] for r in many)
+    return {"kind": "reference" if use_ref else "port", "steps_timed": nsteps,
+            "one_thread": {"value": v1, "unit": UNIT, "cores": 1,
+                           "projected_1000_steps_s": 1000 * one[2] / one[1]},
+            "nproc": {"value": vn, "unit": UNIT, "cores": nproc,
+                      "note": "one independent copy per core (the reference's host build runs one simulation "
+                              "on one thread)"}}
 
 
 def run_reference(a):
-    """The reference arm: the reference's CPU code on every host core."""
+    """The reference arm: the reference's CPU code on the host cores, on the
+    same ensemble workload (a bounded sample, see cpu_throughput)."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
-    cpu = cpu_throughput(nsteps=max(1, a.steps), warmup=max(1, a.warmup))
+    cpu = cpu_throughput()
     line = {"metric": METRIC, "value": cpu["value"], "unit": UNIT, "n_gpus": a.gpus, "steps": a.steps,
-            "warmup": a.warmup, "ms_per_step": cpu["elapsed_s"] * 1e3 / max(1, a.steps),
+            "warmup": a.warmup, "ms_per_step": None,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic",
-            "config": dict(workload_config(a.gpus), precision="fp64 (the reference computes in FP64 only)"),
+            "config": dict(workload_config(a.gpus), precision="fp64 (the reference computes in FP64 only)",
+                           same_config=True),
             "impl": "reference",
             "cpu_baseline": {"value": cpu["value"], "unit": UNIT, "cores": cpu["cores"], "kind": cpu["kind"],
                              "sample": cpu["sample"]},
+            "per_side_rate_one_core": cpu["per_side_rate_one_core"],
             "e2e": {"value": cpu["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
     return 0
@@ -406,24 +457,32 @@ def run_e2e_batched(probs, prec, ctx, steps):
             "h2d_bytes_per_step": (nbytes + mbytes) / steps, "d2h_bytes_per_step": nbytes / steps}
 
 
-def accuracy_study(prob, steps: int, device: int):
-    """Per-field relative L2 (inner cells) of the mixed and the FP64-FMA
-    states against the FMA-free FP64 build after `steps` RK4 steps, under the
-    reference's dt rule and at a fixed dt."""
+def field_errors(w, ref, nw):
+    """Per-field error over the inner cells: relative L2 ||x - y|| / ||y||; a
+    field whose reference norm is zero or below 1e-9 of the largest field
+    norm takes its absolute L2 over the largest field norm instead."""
     import numpy as np
+    sl = (slice(0, nw),) + (slice(2, -2),) * (w.ndim - 1)
+    x, y = w[sl], ref[sl]
+    norms = np.array([np.linalg.norm(y[f]) for f in range(nw)])
+    big = norms.max()
+    return [float(np.linalg.norm(x[f] - y[f]) / (norms[f] if norms[f] > 1e-9 * big else big)) for f in range(nw)]
 
+
+def accuracy_study(prob, steps: int, device: int, modes=("dt_rule", "fixed_dt"), dt_probe_steps: int | None = None):
+    """Per-field errors (field_errors) of the mixed and the FP64-FMA states
+    against the FMA-free FP64 build (bit-identical to the oracle) after
+    `steps` RK4 steps, under the reference's dt rule and at a fixed dt (half
+    the dt the rule reaches after min(steps, dt_probe_steps) steps)."""
     from smaug_b200 import PREC_MIXED, Engine
-
-    def rel(w, ref, nw):
-        sl = (slice(0, nw),) + (slice(2, -2),) * (w.ndim - 1)
-        x, y = w[sl], ref[sl]
-        norms = np.array([np.linalg.norm(y[f]) for f in range(nw)])
-        return [float(np.linalg.norm(x[f] - y[f]) / (norms[f] if norms[f] > 0 else norms.max())) for f in range(nw)]
 
     nw = 2 + 2 * prob.ndim
     out = {"steps": steps, "reference": "FP64 FMA-free build (bit-identical to the oracle)"}
-    dt_fixed = None
-    for mode in ("dt_rule", "fixed_dt"):
+    probe = Engine(prob, rk4=True, device=device)
+    probe.step(min(steps, dt_probe_steps or steps))
+    dt_fixed = 0.5 * probe.scalars()["dt"]
+    probe.close()
+    for mode in modes:
         kw = {"dt_mode": 1} if mode == "dt_rule" else {"dt_mode": 0, "dt0": dt_fixed}
         ex = Engine(prob, rk4=True, exact=True, device=device, **kw)
         fa = Engine(prob, rk4=True, device=device, **kw)
@@ -431,14 +490,48 @@ def accuracy_study(prob, steps: int, device: int):
         for e in (ex, fa, mi):
             e.step(steps)
         we = ex.state()
-        rm, rf = rel(mi.state(), we, nw), rel(fa.state(), we, nw)
-        out[mode] = {"mixed_max_rel_l2": max(rm), "mixed_rel_l2_per_field": rm, "fp64_fma_max_rel_l2": max(rf)}
-        if mode == "dt_rule":
-            dt_fixed = 0.5 * ex.scalars()["dt"]
-        else:
+        rm, rf = field_errors(mi.state(), we, nw), field_errors(fa.state(), we, nw)
+        out[mode] = {"mixed_max_rel_l2": max(rm), "mixed_rel_l2_per_field": rm, "fp64_fma_max_rel_l2": max(rf),
+                     "meets_1e-5": max(rm) <= 1e-5}
+        if mode == "fixed_dt":
             out[mode]["dt"] = dt_fixed
         for e in (ex, fa, mi):
             e.close()
+    return out
+
+
+def run_c1(a, ctx):
+    """the Orszag-Tang vortex 256^2, periodic, hyperdiffusion on,
+    Courant 0.3, 1000 RK4 steps under the reference's dt rule, on the GPU
+    through the single-simulation context (FP64 and mixed, CUDA events around
+    the 1000 steps); the reference's CPU build on the same problem (a bounded
+    sample at 1 thread and on every core); and the accuracy of 1000 steps,
+    mixed and FP64-FMA against the FMA-free FP64 build, at a fixed dt and
+    under the dt rule."""
+    import torch
+
+    from smaug_b200 import PREC_FP64, PREC_MIXED, Engine, problems
+    prob = problems.orszag_tang(256)
+    n_int = prob.interior
+    out = {"workload": "Orszag-Tang 256^2 interior, periodic, gamma 5/3, hyperdiffusion on, Courant 0.3, "
+                       "dt rule (moddton), RK4", "steps": a.c1_steps}
+    for name, prec in (("fp64", PREC_FP64), ("mixed", PREC_MIXED)):
+        e = Engine(prob, rk4=True, precision=prec, device=ctx.local)
+        e.step(max(3, a.warmup))
+        e.sync()
+        e.set_state(prob.w)  # the timed run starts from the initial state
+        ms = ctx.max_ms(event_ms(torch.cuda.ExternalStream(e.stream), lambda: e.step(a.c1_steps)))
+        e.sync()
+        out[name] = {"value": ctx.world * n_int * a.c1_steps / (ms / 1e3), "unit": UNIT, "wall_ms": ms,
+                     "final_dt": e.scalars()["dt"]}
+        e.close()
+    if ctx.rank == 0 and ctx.world == 1 and not a.no_cpu_baseline:
+        try:
+            out["cpu_reference"] = cpu_c1()
+        except Exception as ex:  # the GPU numbers stand on their own
+            out["cpu_reference"] = {"failed": str(ex)}
+    if a.accuracy_steps > 0 and ctx.rank == 0:
+        out["accuracy_1000_steps"] = accuracy_study(prob, a.c1_steps, ctx.local, dt_probe_steps=50)
     return out
 
 
@@ -491,6 +584,9 @@ def run_blast(a, ctx):
     out["mixed_vs_fp64"] = out["mixed"]["value"] / out["fp64"]["value"]
     if a.accuracy_steps > 0 and ctx.rank == 0:
         out["accuracy"] = accuracy_study(prob, a.accuracy_steps, ctx.local)
+        if a.c2_accuracy_steps > 0:  # configs[1]: 500 steps at a fixed dt
+            out["accuracy_500_steps_fixed_dt"] = accuracy_study(prob, a.c2_accuracy_steps, ctx.local,
+                                                                modes=("fixed_dt",), dt_probe_steps=50)
     return out
 
 
@@ -597,7 +693,11 @@ def main():
     ap.add_argument("--serve-requests", type=int, default=48,
                     help="requests of the serving stream (0: skip); the full stream is 2000")
     ap.add_argument("--accuracy-steps", type=int, default=50,
-                    help="steps of the blast-wave accuracy study against the FP64 oracle build (0: skip)")
+                    help="steps of the blast-wave accuracy study against the FP64 oracle build (0: skip all "
+                         "accuracy studies)")
+    ap.add_argument("--c1-steps", type=int, default=1000, help="RK4 steps of the Orszag-Tang 256^2 line (0: skip)")
+    ap.add_argument("--c2-accuracy-steps", type=int, default=500,
+                    help="steps of the blast-wave fixed-dt accuracy study (0: skip)")
     a = ap.parse_args()
     if a.impl == "reference":
         return run_reference(a)
@@ -628,6 +728,8 @@ def main():
                                                         "another (smaug_create / smaug_step)")
             line_extra["batched_vs_plain_fp64"] = head["value"] / plain["value"]
         e2e = run_e2e_batched(probs, PREC_MIXED, ctx, K)
+        if a.c1_steps > 0:
+            line_extra["c1_ot256"] = run_c1(a, ctx)
         if not a.no_blast:
             line_extra["blast128"] = run_blast(a, ctx)
         if not a.no_atmos3d:
@@ -651,7 +753,7 @@ def main():
     cpu = None
     if ctx.rank == 0 and ctx.world == 1 and not a.no_cpu_baseline and not a.only_batched:
         try:
-            cpu = cpu_throughput(nsteps=2, warmup=1)
+            cpu = cpu_throughput()
             cpu = {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")}
         except Exception as ex:  # the GPU number stands on its own
             cpu = {"value": None, "unit": UNIT, "cores": 0, "kind": "reference", "sample": f"failed: {ex}"}
