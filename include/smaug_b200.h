@@ -281,10 +281,15 @@ int smaug_batch_destroy(smaug_batch *b);
  * Returns SMAUG_ERR_FULL when no slot or no arena block is free, and
  * SMAUG_ERR_ARG for a metric that is not a tensor-product grid on the inner
  * cells or has a non-positive entry (checked on the device, in the slot's own
- * memory, which is released again).
+ * memory, which is released again).  The admission runs on a stream of its
+ * own and waits only for its own copies and checks, not for the steps queued
+ * on the batch; the next smaug_batch_step waits for it on the device.
  */
 int smaug_batch_add(smaug_batch *b, const smaug_params *prm, const double *delx, const double *w,
                     long long nsteps, int *slot);
+/* Remove a simulation.  Its slot and arena block become free for a new
+ * admission once the steps and reads queued before the removal are done
+ * (smaug_batch_add waits for them only when nothing else is free). */
 int smaug_batch_remove(smaug_batch *b, int slot);
 
 /* Enqueue nsteps batch steps (asynchronous). */
@@ -295,6 +300,26 @@ int smaug_batch_poll(smaug_batch *b, long long *steps_left, int n);
 
 /* Wait; returns the first simulation error (its slot in *bad_slot, may be NULL). */
 int smaug_batch_sync(smaug_batch *b, int *bad_slot);
+
+/*
+ * Polling and read-back that do not wait for later steps, for a serving loop
+ * that keeps the next steps queued while it handles the last ones:
+ *   smaug_batch_poll_begin   snapshot of the steps left per slot behind the
+ *                            steps queued so far (*ticket names it; up to 4
+ *                            snapshots wait at a time)
+ *   smaug_batch_poll_end     wait for that snapshot only and return it (as
+ *                            smaug_batch_poll; -1 for a free slot)
+ *   smaug_batch_get_state_async
+ *                            queue the read of a simulation that had finished
+ *                            in the last snapshot waited for, on a read-back
+ *                            stream that follows that snapshot (not the steps
+ *                            queued after it); w is best pinned host memory
+ *   smaug_batch_io_wait      wait for the queued reads
+ */
+int smaug_batch_poll_begin(smaug_batch *b, long long *ticket);
+int smaug_batch_poll_end(smaug_batch *b, long long ticket, long long *steps_left, int n);
+int smaug_batch_get_state_async(smaug_batch *b, int slot, double *w, size_t count);
+int smaug_batch_io_wait(smaug_batch *b);
 
 /* One simulation's state (NVAR * N doubles) and scalars (as smaug_get_scalars). */
 int smaug_batch_get_state(smaug_batch *b, int slot, double *w, size_t count);

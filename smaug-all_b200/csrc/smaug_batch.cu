@@ -85,10 +85,30 @@ size_t sim_footprint(const SimPlan &p) {
 
 struct Slot {
   bool used = false;
+  bool pending = false;  // removed, but queued work may still read its slot and block
   size_t off = 0, bytes = 0;
   SimPlan plan;
   long long steps_total = 0;
 };
+
+// A removed simulation's arena block and slot, released once the work queued
+// before the removal (on the step stream and the read-back stream) is done.
+struct Pending {
+  size_t off = 0, bytes = 0;
+  int slot = -1;
+  cudaEvent_t ev_main = nullptr, ev_io = nullptr;
+};
+
+constexpr int kSnaps = 4;  // poll snapshots in flight
+
+// Per slot: the steps it has left and its status (set at admission, on the
+// upload stream, by a kernel: its arguments are copied at launch).
+__global__ void set_slot_kernel(long long *left, int *status, int slot, long long nsteps) {
+  if (threadIdx.x == 0 && blockIdx.x == 0) {
+    left[slot] = nsteps;
+    status[slot] = 0;
+  }
+}
 
 }  // namespace
 
@@ -120,6 +140,27 @@ struct smaug_batch {
   std::vector<cudaEvent_t> ev;
   size_t ev_used = 0;
   std::string err;
+  // Admissions run on `up`, asynchronous state reads on `io`, so that neither
+  // waits for the steps queued on `stream`; the step stream waits for the
+  // admissions before its next launch (up_done).
+  cudaStream_t up = nullptr, io = nullptr;
+  cudaEvent_t up_done = nullptr;
+  bool up_dirty = false;
+  std::vector<Pending> pending;
+  std::vector<cudaEvent_t> ev_pool;
+  // poll snapshots: steps left per slot, copied into pinned memory behind the
+  // steps queued so far (ticket t uses ring entry t % kSnaps)
+  long long *snap_h[kSnaps] = {};
+  cudaEvent_t snap_ev[kSnaps] = {};
+  long long snap_ticket[kSnaps] = {-1, -1, -1, -1};
+  long long next_ticket = 0;
+  int last_snap = -1;  // ring entry of the last snapshot waited for (asynchronous reads follow it)
+  // pinned staging of the work lists and the table (two sets, used in turn)
+  BatchInst *st_tab[2] = {};
+  WorkItem *st_work[2] = {}, *st_gwork[2] = {};
+  size_t st_work_cap[2] = {}, st_gwork_cap[2] = {};
+  cudaEvent_t st_ev[2] = {};
+  int st_cur = 0;
 };
 
 namespace {
@@ -179,6 +220,21 @@ void set_tiles(const smaug_batch *b, BatchInst &I) {
 
 // Rebuild the work list and the persistent grid for the current simulations
 // and tile shape.
+// Grow pinned staging buffer k of `what` (its copies from two rebuilds ago
+// are done: the caller waited for st_ev[k]).
+int stage_grow(smaug_batch *b, WorkItem **buf, size_t *cap, size_t need) {
+  if (need <= *cap) return SMAUG_OK;
+  if (*buf) cudaFreeHost(*buf);
+  *buf = nullptr;
+  *cap = std::max(need, (size_t)1024) * 2;
+  BK(cudaMallocHost((void **)buf, sizeof(WorkItem) * *cap));
+  return SMAUG_OK;
+}
+
+// Rebuild the work list and the persistent grid for the current simulations
+// and tile shape.  The table and the lists go to the device from pinned
+// staging buffers (two sets, used in turn), so nothing here waits for the
+// steps already queued, except when a device list must grow.
 int rebuild(smaug_batch *b) {
   std::vector<WorkItem> w, gw;
   for (int i = 0; i < b->max_inst; ++i) {
@@ -191,32 +247,84 @@ int rebuild(smaug_batch *b) {
     const long long ng = ghost_cells(b->h_tab[i].geo, b->D);
     for (long long t = 0; t < (ng + 255) / 256; ++t) gw.push_back({i, (int)t, 0, 0});
   }
-  if (gw.size() > b->gwork_cap) {
+  if (gw.size() > b->gwork_cap || w.size() > b->work_cap) {  // queued steps read the device lists
     BK(cudaStreamSynchronize(b->stream));
-    if (b->d_gwork) cudaFree(b->d_gwork);
-    b->gwork_cap = std::max(gw.size(), (size_t)1024) * 2;
-    BK(cudaMalloc(&b->d_gwork, sizeof(WorkItem) * b->gwork_cap));
+    if (gw.size() > b->gwork_cap) {
+      if (b->d_gwork) cudaFree(b->d_gwork);
+      b->gwork_cap = std::max(gw.size(), (size_t)1024) * 2;
+      BK(cudaMalloc(&b->d_gwork, sizeof(WorkItem) * b->gwork_cap));
+    }
+    if (w.size() > b->work_cap) {
+      if (b->d_work) cudaFree(b->d_work);
+      b->work_cap = std::max(w.size(), (size_t)1024) * 2;
+      BK(cudaMalloc(&b->d_work, sizeof(WorkItem) * b->work_cap));
+    }
   }
+  const int k = b->st_cur;
+  b->st_cur ^= 1;
+  BK(cudaEventSynchronize(b->st_ev[k]));  // the copies out of set k, two rebuilds ago
+  int rc = stage_grow(b, &b->st_gwork[k], &b->st_gwork_cap[k], gw.size());
+  if (rc != SMAUG_OK) return rc;
+  rc = stage_grow(b, &b->st_work[k], &b->st_work_cap[k], w.size());
+  if (rc != SMAUG_OK) return rc;
+  std::memcpy(b->st_tab[k], b->h_tab.data(), sizeof(BatchInst) * b->max_inst);
+  if (!gw.empty()) std::memcpy(b->st_gwork[k], gw.data(), sizeof(WorkItem) * gw.size());
+  if (!w.empty()) std::memcpy(b->st_work[k], w.data(), sizeof(WorkItem) * w.size());
   if (!gw.empty())
-    BK(cudaMemcpyAsync(b->d_gwork, gw.data(), sizeof(WorkItem) * gw.size(), cudaMemcpyHostToDevice, b->stream));
+    BK(cudaMemcpyAsync(b->d_gwork, b->st_gwork[k], sizeof(WorkItem) * gw.size(), cudaMemcpyHostToDevice, b->stream));
+  BK(cudaMemcpyAsync(b->d_tab, b->st_tab[k], sizeof(BatchInst) * b->max_inst, cudaMemcpyHostToDevice, b->stream));
+  if (!w.empty())
+    BK(cudaMemcpyAsync(b->d_work, b->st_work[k], sizeof(WorkItem) * w.size(), cudaMemcpyHostToDevice, b->stream));
+  BK(cudaEventRecord(b->st_ev[k], b->stream));
   b->ngwork = (int)gw.size();
   b->ggrid = std::min(b->ngwork, 148 * 8);
-  BK(cudaMemcpyAsync(b->d_tab, b->h_tab.data(), sizeof(BatchInst) * b->max_inst, cudaMemcpyHostToDevice, b->stream));
-  if (w.size() > b->work_cap) {
-    BK(cudaStreamSynchronize(b->stream));
-    if (b->d_work) cudaFree(b->d_work);
-    b->work_cap = std::max(w.size(), (size_t)1024) * 2;
-    BK(cudaMalloc(&b->d_work, sizeof(WorkItem) * b->work_cap));
-  }
-  if (!w.empty())
-    BK(cudaMemcpyAsync(b->d_work, w.data(), sizeof(WorkItem) * w.size(), cudaMemcpyHostToDevice, b->stream));
-  // the copy source is pageable host memory: wait for it before w goes away
-  BK(cudaStreamSynchronize(b->stream));
   b->nwork = (int)w.size();
   const int occ = std::max(1, smaug_batchk::batch_stage_occupancy(b->D, b->mixed, b->variant));
   b->grid = std::min(b->nwork, occ * b->sms);
   drop_graphs(b);
   b->dirty = false;
+  return SMAUG_OK;
+}
+
+// The step stream waits for the admissions queued on the upload stream.
+int join_uploads(smaug_batch *b) {
+  if (!b->up_dirty) return SMAUG_OK;
+  BK(cudaEventRecord(b->up_done, b->up));
+  BK(cudaStreamWaitEvent(b->stream, b->up_done, 0));
+  b->up_dirty = false;
+  return SMAUG_OK;
+}
+
+cudaEvent_t pool_event(smaug_batch *b) {
+  if (!b->ev_pool.empty()) {
+    cudaEvent_t e = b->ev_pool.back();
+    b->ev_pool.pop_back();
+    return e;
+  }
+  cudaEvent_t e = nullptr;
+  if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) return nullptr;
+  return e;
+}
+
+// Release the blocks and slots of removed simulations whose queued work is
+// done (wait: also those whose work is still queued, waiting for it).
+int reclaim(smaug_batch *b, bool wait) {
+  for (size_t i = 0; i < b->pending.size();) {
+    Pending &q = b->pending[i];
+    if (wait) {
+      BK(cudaEventSynchronize(q.ev_main));
+      BK(cudaEventSynchronize(q.ev_io));
+    } else if (cudaEventQuery(q.ev_main) != cudaSuccess || cudaEventQuery(q.ev_io) != cudaSuccess) {
+      ++i;
+      continue;
+    }
+    arena_free(b, q.off, q.bytes);
+    b->slots[q.slot].pending = false;
+    b->ev_pool.push_back(q.ev_main);
+    b->ev_pool.push_back(q.ev_io);
+    b->pending.erase(b->pending.begin() + i);
+  }
+  cudaGetLastError();  // a not-ready query leaves no error behind
   return SMAUG_OK;
 }
 
@@ -291,6 +399,17 @@ int smaug_batch_create(int ndim, int precision, int device, size_t arena_bytes, 
   b->sms = sms > 0 ? sms : 148;
   BK(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking));
   BK(cudaStreamCreateWithFlags(&b->cap, cudaStreamNonBlocking));
+  BK(cudaStreamCreateWithFlags(&b->up, cudaStreamNonBlocking));
+  BK(cudaStreamCreateWithFlags(&b->io, cudaStreamNonBlocking));
+  BK(cudaEventCreateWithFlags(&b->up_done, cudaEventDisableTiming));
+  for (int k = 0; k < kSnaps; ++k) {
+    BK(cudaMallocHost((void **)&b->snap_h[k], sizeof(long long) * max_sims));
+    BK(cudaEventCreateWithFlags(&b->snap_ev[k], cudaEventDisableTiming));
+  }
+  for (int k = 0; k < 2; ++k) {
+    BK(cudaMallocHost((void **)&b->st_tab[k], sizeof(BatchInst) * max_sims));
+    BK(cudaEventCreateWithFlags(&b->st_ev[k], cudaEventDisableTiming));
+  }
   BK(cudaMalloc(&b->arena, b->arena_bytes));
   b->free_[0] = b->arena_bytes;
   BK(cudaMalloc(&b->d_tab, sizeof(BatchInst) * max_sims));
@@ -307,6 +426,8 @@ int smaug_batch_destroy(smaug_batch *b) {
   if (!b) return SMAUG_OK;
   cudaSetDevice(b->device);
   if (b->stream) cudaStreamSynchronize(b->stream);
+  if (b->up) cudaStreamSynchronize(b->up);
+  if (b->io) cudaStreamSynchronize(b->io);
   drop_graphs(b);
   for (auto e : b->ev) cudaEventDestroy(e);
   cudaFree(b->arena);
@@ -315,8 +436,26 @@ int smaug_batch_destroy(smaug_batch *b) {
   cudaFree(b->d_status);
   cudaFree(b->d_work);
   cudaFree(b->d_gwork);
+  for (auto &q : b->pending) {
+    if (q.ev_main) cudaEventDestroy(q.ev_main);
+    if (q.ev_io) cudaEventDestroy(q.ev_io);
+  }
+  for (auto e : b->ev_pool) cudaEventDestroy(e);
+  for (int k = 0; k < kSnaps; ++k) {
+    if (b->snap_h[k]) cudaFreeHost(b->snap_h[k]);
+    if (b->snap_ev[k]) cudaEventDestroy(b->snap_ev[k]);
+  }
+  for (int k = 0; k < 2; ++k) {
+    if (b->st_tab[k]) cudaFreeHost(b->st_tab[k]);
+    if (b->st_work[k]) cudaFreeHost(b->st_work[k]);
+    if (b->st_gwork[k]) cudaFreeHost(b->st_gwork[k]);
+    if (b->st_ev[k]) cudaEventDestroy(b->st_ev[k]);
+  }
+  if (b->up_done) cudaEventDestroy(b->up_done);
   if (b->stream) cudaStreamDestroy(b->stream);
   if (b->cap) cudaStreamDestroy(b->cap);
+  if (b->up) cudaStreamDestroy(b->up);
+  if (b->io) cudaStreamDestroy(b->io);
   delete b;
   return SMAUG_OK;
 }
@@ -334,16 +473,25 @@ int smaug_batch_add(smaug_batch *b, const smaug_params *prm, const double *delx,
   // one line per dim here; the metric itself is checked on the device below
   std::vector<double> d1(p.geo.n[0] + p.geo.n[1] + p.geo.n[2]);
   metric_lines_host(p, delx, d1.data());
-  int slot = -1;
-  for (int i = 0; i < b->max_inst; ++i)
-    if (!b->slots[i].used) {
-      slot = i;
-      break;
-    }
-  if (slot < 0) return bfail(b, SMAUG_ERR_FULL, "no free simulation slot");
+  BK(cudaSetDevice(b->device));
+  // a slot and a block: first from what is free now, then, if removed
+  // simulations still wait for their queued work, after waiting for it
   const size_t fp = sim_footprint(p);
+  int slot = -1;
   size_t off = 0;
-  if (!arena_alloc(b, fp, &off)) return bfail(b, SMAUG_ERR_FULL, "arena has no free block of the simulation's footprint");
+  for (int attempt = 0; attempt < 2 && slot < 0; ++attempt) {
+    const int rc = reclaim(b, attempt == 1);
+    if (rc != SMAUG_OK) return rc;
+    int cand = -1;
+    for (int i = 0; i < b->max_inst; ++i)
+      if (!b->slots[i].used && !b->slots[i].pending) {
+        cand = i;
+        break;
+      }
+    if (cand >= 0 && arena_alloc(b, fp, &off)) slot = cand;
+    if (b->pending.empty()) break;
+  }
+  if (slot < 0) return bfail(b, SMAUG_ERR_FULL, "no free simulation slot or arena block of the simulation's footprint");
   // every return below that does not admit the simulation releases its block
   // (stream order keeps a later admission's uploads behind any copy queued here)
   struct BlockGuard {
@@ -354,7 +502,6 @@ int smaug_batch_add(smaug_batch *b, const smaug_params *prm, const double *delx,
       if (!keep) arena_free(b, off, bytes);
     }
   } guard{b, off, fp};
-  BK(cudaSetDevice(b->device));
   // carve
   char *q = b->arena + off;
   auto take = [&](size_t bytes) {
@@ -396,7 +543,10 @@ int smaug_batch_add(smaug_batch *b, const smaug_params *prm, const double *delx,
   I.bg = bg;
   I.sc = sc;
   I.active = 1;
-  cudaStream_t s = b->stream;
+  // the admission's own stream: it neither waits for the queued steps nor
+  // touches their memory (the slot and the block are not referenced by any of
+  // them); the step stream waits for it before its next launch
+  cudaStream_t s = b->up;
   // The full metric goes to a stage buffer that nothing uses before the
   // first step (mixed F[2]: NW >= 2 D floats per cell; FP64 W[1]) for its
   // check; the last dim's array stays as dxlast.
@@ -438,10 +588,9 @@ int smaug_batch_add(smaug_batch *b, const smaug_params *prm, const double *delx,
   }
   p.phys.has_bgb = chk[1];
   I.phys = p.phys;
-  BK(cudaMemcpyAsync(b->d_left + slot, &nsteps, sizeof(long long), cudaMemcpyHostToDevice, s));
-  const int zero = 0;
-  BK(cudaMemcpyAsync(b->d_status + slot, &zero, sizeof(int), cudaMemcpyHostToDevice, s));
-  BK(cudaStreamSynchronize(s));
+  set_slot_kernel<<<1, 1, 0, s>>>(b->d_left, b->d_status, slot, nsteps);
+  BK(cudaGetLastError());
+  b->up_dirty = true;
   guard.keep = true;
   Slot &S = b->slots[slot];
   S.used = true;
@@ -458,11 +607,23 @@ int smaug_batch_add(smaug_batch *b, const smaug_params *prm, const double *delx,
 int smaug_batch_remove(smaug_batch *b, int slot) {
   if (!b || slot < 0 || slot >= b->max_inst || !b->slots[slot].used) return SMAUG_ERR_ARG;
   BK(cudaSetDevice(b->device));
-  // queued steps may still use the slot's memory: stream order keeps a later
-  // simulation's uploads behind them
+  // Steps queued before now, and state reads queued on the read-back stream,
+  // may still read the slot's table entry, its steps-left counter and its
+  // block: both are released once that work is done (reclaim, at the next
+  // admission).  Later steps no longer include the simulation.
+  Pending q;
+  q.off = b->slots[slot].off;
+  q.bytes = b->slots[slot].bytes;
+  q.slot = slot;
+  q.ev_main = pool_event(b);
+  q.ev_io = pool_event(b);
+  if (!q.ev_main || !q.ev_io) return bfail(b, SMAUG_ERR_CUDA, "no CUDA event for a removal");
+  BK(cudaEventRecord(q.ev_main, b->stream));
+  BK(cudaEventRecord(q.ev_io, b->io));
+  b->pending.push_back(q);
   b->h_tab[slot] = BatchInst{};
-  arena_free(b, b->slots[slot].off, b->slots[slot].bytes);
   b->slots[slot] = Slot{};
+  b->slots[slot].pending = true;
   b->dirty = true;
   return SMAUG_OK;
 }
@@ -470,6 +631,10 @@ int smaug_batch_remove(smaug_batch *b, int slot) {
 int smaug_batch_step(smaug_batch *b, int nsteps) {
   if (!b || nsteps < 0) return SMAUG_ERR_ARG;
   BK(cudaSetDevice(b->device));
+  {
+    const int rc = join_uploads(b);
+    if (rc != SMAUG_OK) return rc;
+  }
   if (b->dirty) {
     int rc = rebuild(b);
     if (rc != SMAUG_OK) return rc;
@@ -503,6 +668,10 @@ int smaug_batch_step(smaug_batch *b, int nsteps) {
 int smaug_batch_poll(smaug_batch *b, long long *steps_left, int n) {
   if (!b || !steps_left || n < b->max_inst) return SMAUG_ERR_ARG;
   BK(cudaSetDevice(b->device));
+  {
+    const int rc_ = join_uploads(b);
+    if (rc_ != SMAUG_OK) return rc_;
+  }
   BK(cudaMemcpyAsync(steps_left, b->d_left, sizeof(long long) * b->max_inst, cudaMemcpyDeviceToHost, b->stream));
   BK(cudaStreamSynchronize(b->stream));
   for (int i = 0; i < b->max_inst; ++i)
@@ -510,10 +679,74 @@ int smaug_batch_poll(smaug_batch *b, long long *steps_left, int n) {
   return SMAUG_OK;
 }
 
+int smaug_batch_poll_begin(smaug_batch *b, long long *ticket) {
+  if (!b || !ticket) return SMAUG_ERR_ARG;
+  BK(cudaSetDevice(b->device));
+  {
+    const int rc_ = join_uploads(b);
+    if (rc_ != SMAUG_OK) return rc_;
+  }
+  const long long t = b->next_ticket;
+  const int k = (int)(t % kSnaps);
+  if (b->snap_ticket[k] >= 0) return bfail(b, SMAUG_ERR_STATE, "more than 4 poll snapshots waiting: end one first");
+  BK(cudaMemcpyAsync(b->snap_h[k], b->d_left, sizeof(long long) * b->max_inst, cudaMemcpyDeviceToHost, b->stream));
+  BK(cudaEventRecord(b->snap_ev[k], b->stream));
+  b->snap_ticket[k] = t;
+  b->next_ticket = t + 1;
+  *ticket = t;
+  return SMAUG_OK;
+}
+
+int smaug_batch_poll_end(smaug_batch *b, long long ticket, long long *steps_left, int n) {
+  if (!b || !steps_left || n < b->max_inst || ticket < 0) return SMAUG_ERR_ARG;
+  const int k = (int)(ticket % kSnaps);
+  if (b->snap_ticket[k] != ticket) return bfail(b, SMAUG_ERR_STATE, "no such poll snapshot waiting");
+  BK(cudaSetDevice(b->device));
+  BK(cudaEventSynchronize(b->snap_ev[k]));
+  std::memcpy(steps_left, b->snap_h[k], sizeof(long long) * b->max_inst);
+  for (int i = 0; i < b->max_inst; ++i)
+    if (!b->slots[i].used) steps_left[i] = -1;
+  b->snap_ticket[k] = -1;
+  b->last_snap = k;
+  return SMAUG_OK;
+}
+
+int smaug_batch_get_state_async(smaug_batch *b, int slot, double *w, size_t count) {
+  if (!b || !w || slot < 0 || slot >= b->max_inst || !b->slots[slot].used) return SMAUG_ERR_ARG;
+  if (b->last_snap < 0) return bfail(b, SMAUG_ERR_STATE, "smaug_batch_get_state_async follows smaug_batch_poll_end");
+  const SimPlan &p = b->slots[slot].plan;
+  const BatchInst &I = b->h_tab[slot];
+  const long long N = p.geo.N;
+  if (count != (size_t)p.NVAR * (size_t)N) return bfail(b, SMAUG_ERR_ARG, "state must hold NVAR * N doubles");
+  BK(cudaSetDevice(b->device));
+  // after the steps the last waited-for snapshot followed; the steps queued
+  // since do not write a simulation that had finished by then
+  BK(cudaStreamWaitEvent(b->io, b->snap_ev[b->last_snap], 0));
+  if (p.mixed) {
+    combine_kernel<<<148 * 4, 256, 0, b->io>>>(I.F[0], I.F[1], I.W[0], (long long)p.NW * N);
+    b->launches++;
+    BK(cudaGetLastError());
+  }
+  BK(cudaMemcpyAsync(w, I.W[0], sizeof(double) * p.NW * N, cudaMemcpyDeviceToHost, b->io));
+  BK(cudaMemcpyAsync(w + (size_t)p.NW * N, I.bg, sizeof(double) * p.NB * N, cudaMemcpyDeviceToHost, b->io));
+  return SMAUG_OK;
+}
+
+int smaug_batch_io_wait(smaug_batch *b) {
+  if (!b) return SMAUG_ERR_ARG;
+  BK(cudaSetDevice(b->device));
+  BK(cudaStreamSynchronize(b->io));
+  return SMAUG_OK;
+}
+
 int smaug_batch_sync(smaug_batch *b, int *bad_slot) {
   if (!b) return SMAUG_ERR_ARG;
   if (bad_slot) *bad_slot = -1;
   BK(cudaSetDevice(b->device));
+  {
+    const int rc_ = join_uploads(b);
+    if (rc_ != SMAUG_OK) return rc_;
+  }
   std::vector<int> st(b->max_inst);
   BK(cudaMemcpyAsync(st.data(), b->d_status, sizeof(int) * b->max_inst, cudaMemcpyDeviceToHost, b->stream));
   BK(cudaStreamSynchronize(b->stream));
@@ -532,6 +765,10 @@ int smaug_batch_get_state(smaug_batch *b, int slot, double *w, size_t count) {
   const long long N = p.geo.N;
   if (count != (size_t)p.NVAR * (size_t)N) return bfail(b, SMAUG_ERR_ARG, "state must hold NVAR * N doubles");
   BK(cudaSetDevice(b->device));
+  {
+    const int rc_ = join_uploads(b);
+    if (rc_ != SMAUG_OK) return rc_;
+  }
   if (p.mixed) {
     combine_kernel<<<148 * 8, 256, 0, b->stream>>>(I.F[0], I.F[1], I.W[0], (long long)p.NW * N);
     b->launches++;
@@ -546,6 +783,10 @@ int smaug_batch_get_state(smaug_batch *b, int slot, double *w, size_t count) {
 int smaug_batch_get_scalars(smaug_batch *b, int slot, double out[8]) {
   if (!b || !out || slot < 0 || slot >= b->max_inst || !b->slots[slot].used) return SMAUG_ERR_ARG;
   BK(cudaSetDevice(b->device));
+  {
+    const int rc_ = join_uploads(b);
+    if (rc_ != SMAUG_OK) return rc_;
+  }
   DevScalars s;
   long long left = 0;
   BK(cudaMemcpyAsync(&s, b->h_tab[slot].sc, sizeof(DevScalars), cudaMemcpyDeviceToHost, b->stream));
@@ -563,6 +804,10 @@ int smaug_batch_get_scalars(smaug_batch *b, int slot, double out[8]) {
 int smaug_batch_tune(smaug_batch *b, int reps, int *variant_out, double *ms_out, int nms) {
   if (!b || reps < 1) return SMAUG_ERR_ARG;
   BK(cudaSetDevice(b->device));
+  {
+    const int rc_ = join_uploads(b);
+    if (rc_ != SMAUG_OK) return rc_;
+  }
   const int nv = b->D == 2 ? kBatchVariants2 : kBatchVariants3;
   cudaEvent_t e0, e1;
   BK(cudaEventCreate(&e0));

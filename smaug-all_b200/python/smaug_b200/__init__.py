@@ -86,6 +86,10 @@ def load_library(path: Path | None = None):
     L.smaug_batch_step.argtypes = [_VP, _I]
     L.smaug_batch_poll.argtypes = [_VP, ctypes.POINTER(_LL), _I]
     L.smaug_batch_sync.argtypes = [_VP, ctypes.POINTER(_I)]
+    L.smaug_batch_poll_begin.argtypes = [_VP, ctypes.POINTER(_LL)]
+    L.smaug_batch_poll_end.argtypes = [_VP, _LL, ctypes.POINTER(_LL), _I]
+    L.smaug_batch_get_state_async.argtypes = [_VP, _I, _PD, _SZ]
+    L.smaug_batch_io_wait.argtypes = [_VP]
     L.smaug_batch_get_state.argtypes = [_VP, _I, _PD, _SZ]
     L.smaug_batch_get_scalars.argtypes = [_VP, _I, _PD]
     L.smaug_batch_tune.argtypes = [_VP, _I, ctypes.POINTER(_I), _PD, _I]

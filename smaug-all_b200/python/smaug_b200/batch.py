@@ -81,6 +81,32 @@ class Batch:
         self._check(self.lib.smaug_batch_poll(self.h, out, self.max_sims), "smaug_batch_poll")
         return np.frombuffer(out, dtype=np.int64).copy()
 
+    def poll_begin(self) -> int:
+        """Snapshot the steps left per slot behind the steps queued so far
+        (does not wait); returns its ticket."""
+        t = ctypes.c_longlong(-1)
+        self._check(self.lib.smaug_batch_poll_begin(self.h, ctypes.byref(t)), "smaug_batch_poll_begin")
+        return t.value
+
+    def poll_end(self, ticket: int) -> np.ndarray:
+        """Wait for snapshot `ticket` only: steps left per slot (-1: free)."""
+        out = (ctypes.c_longlong * self.max_sims)()
+        self._check(self.lib.smaug_batch_poll_end(self.h, ticket, out, self.max_sims), "smaug_batch_poll_end")
+        return np.frombuffer(out, dtype=np.int64).copy()
+
+    def state_async(self, slot: int, out: np.ndarray):
+        """Queue the read of a simulation that had finished in the last snapshot
+        poll_end returned; out (best pinned) is filled by io_wait()."""
+        prob = self.probs[slot]
+        if out.dtype != np.float64 or not out.flags.c_contiguous or out.size != prob.w.size:
+            raise SmaugError("out must be a C-contiguous float64 array of the problem's size")
+        self._check(self.lib.smaug_batch_get_state_async(self.h, slot, out.ctypes.data_as(_PD), out.size),
+                    "smaug_batch_get_state_async")
+        return out
+
+    def io_wait(self):
+        self._check(self.lib.smaug_batch_io_wait(self.h), "smaug_batch_io_wait")
+
     def sync(self):
         bad = ctypes.c_int(-1)
         self._check(self.lib.smaug_batch_sync(self.h, ctypes.byref(bad)), "smaug_batch_sync")

@@ -57,60 +57,122 @@ def poisson_stream(count: int, rate: float, make, seed: int = 777, duration: flo
 
 class Server:
     """Runs a request stream through one batch (any object with the Batch
-    methods add / step / poll / state / remove)."""
+    methods add / step / poll_begin / poll_end / state_async / io_wait /
+    remove).
 
-    def __init__(self, batch, chunk: int = 8, keep_results: bool = True):
+    The device is never left without queued work while any simulation is
+    active: the loop keeps `depth` chunks of `chunk` steps queued, each
+    followed by a snapshot of the steps left (poll_begin).  It then waits for
+    the oldest snapshot only -- the chunks queued behind it keep the GPU busy
+    -- retires the simulations that had finished by it (their states are read
+    on the batch's read-back stream after that snapshot, into pinned buffers,
+    while later chunks run), and admits waiting requests as slots and memory
+    free up (admissions run on their own stream and do not wait for the
+    queued chunks either)."""
+
+    def __init__(self, batch, chunk: int = 8, keep_results: bool = True, depth: int = 2):
         self.batch = batch
         self.chunk = chunk
         self.keep_results = keep_results
+        self.depth = max(1, depth)
+        self._pool: dict = {}
 
-    def run(self, requests, realtime: bool = True, clock=time.perf_counter, sleep=time.sleep) -> dict:
+    def _buffer(self, shape):
+        free = self._pool.setdefault(shape, [])
+        if free:
+            return free.pop()
+        try:
+            import torch
+            if torch.cuda.is_available():
+                return torch.empty(shape, dtype=torch.float64, pin_memory=True).numpy()
+        except Exception:
+            pass
+        return np.empty(shape, dtype=np.float64)
+
+    def run(self, requests, realtime: bool = True, clock=time.perf_counter, sleep=time.sleep,
+            stop_after: float | None = None) -> dict:
+        """Serve `requests` (arrival times in seconds from the start).  With
+        stop_after, no request is admitted and no chunk is queued after that
+        many seconds; the loop then ends once the queued chunks are done, and
+        the statistics cover the requests completed by then (cell_updates
+        counts every step executed, of unfinished simulations too)."""
         reqs = sorted(requests, key=lambda r: r.arrival)
         t0 = clock()
         now = lambda: clock() - t0  # noqa: E731
         queue: deque = deque()
-        active: dict = {}
-        i, steps_done, chunks = 0, 0, 0
-        max_active = 0
-        while i < len(reqs) or queue or active:
+        active: dict = {}     # slot -> request
+        steps_seen: dict = {}  # rid -> steps executed as of the last snapshot
+        inflight: deque = deque()  # (ticket, [(slot, rid)]) in queue order
+        i, chunks, max_active = 0, 0, 0
+        samples = []  # (t, waiting, active)
+        stopped = False
+        while True:
             t = now()
-            while i < len(reqs) and (reqs[i].arrival <= t or not realtime):
+            if stop_after is not None and t >= stop_after:
+                stopped = True
+            while not stopped and i < len(reqs) and (reqs[i].arrival <= t or not realtime):
                 queue.append(reqs[i])
                 i += 1
-            while queue:  # first come first served: the head waits until it fits
+            while queue and not stopped:  # first come first served: the head waits until it fits
                 r = queue[0]
                 slot = self.batch.add(r.prob, r.nsteps)
                 if slot is None:
                     break
                 r.slot, r.admitted = slot, now()
                 active[slot] = r
+                steps_seen[r.rid] = 0
                 queue.popleft()
             max_active = max(max_active, len(active))
+            samples.append((round(t, 3), len(queue), len(active)))
+            if active and not stopped and len(inflight) < self.depth:
+                self.batch.step(self.chunk)
+                chunks += 1
+                inflight.append((self.batch.poll_begin(), [(s_, r_.rid) for s_, r_ in active.items()]))
+                if len(inflight) < self.depth:
+                    continue  # fill the pipeline first
+            if inflight:
+                ticket, snap = inflight.popleft()
+                left = self.batch.poll_end(ticket)
+                done = []
+                for slot, rid in snap:
+                    r = active.get(slot)
+                    if r is None or r.rid != rid:
+                        continue
+                    steps_seen[rid] = r.nsteps - int(left[slot])
+                    if left[slot] == 0:
+                        buf = self._buffer(r.prob.w.shape)
+                        self.batch.state_async(slot, buf)
+                        self.batch.remove(slot)
+                        del active[slot]
+                        done.append((r, buf))
+                if done:
+                    self.batch.io_wait()
+                    td = now()
+                    for r, buf in done:
+                        r.done = td
+                        if self.keep_results:
+                            r.result = buf.copy()
+                        self._pool[r.prob.w.shape].append(buf)
+                continue
+            if stopped or (i >= len(reqs) and not queue and not active):
+                break
             if not active:
                 if queue:
                     raise RuntimeError(f"request {queue[0].rid} does not fit an empty batch")
                 if i < len(reqs) and realtime:
                     sleep(max(0.0, reqs[i].arrival - now()))
-                continue
-            self.batch.step(self.chunk)
-            chunks += 1
-            left = self.batch.poll()
-            for slot, r in list(active.items()):
-                if left[slot] == 0:
-                    res = self.batch.state(slot)
-                    r.done = now()
-                    if self.keep_results:
-                        r.result = res
-                    self.batch.remove(slot)
-                    del active[slot]
-                    steps_done += r.nsteps * r.prob.interior
         wall = now()
-        lat = np.array([r.latency for r in reqs])
-        return {"requests": len(reqs), "wall_s": wall, "chunks": chunks, "max_active": max_active,
-                "cell_updates": steps_done, "cell_updates_per_s": steps_done / wall if wall > 0 else 0.0,
+        fin = [r for r in reqs if r.done is not None]
+        lat = np.array([r.latency for r in fin])
+        cell_updates = sum(steps_seen.get(r.rid, 0) * r.prob.interior for r in reqs)
+        return {"requests": len(reqs), "completed": len(fin), "unfinished_active": len(active),
+                "still_waiting": len(queue) + (len(reqs) - i), "wall_s": wall, "chunks": chunks,
+                "max_active": max_active, "cell_updates": cell_updates,
+                "cell_updates_per_s": cell_updates / wall if wall > 0 else 0.0,
                 "p50_s": float(np.percentile(lat, 50)) if len(lat) else None,
                 "p99_s": float(np.percentile(lat, 99)) if len(lat) else None,
-                "mean_s": float(lat.mean()) if len(lat) else None}
+                "mean_s": float(lat.mean()) if len(lat) else None,
+                "queue_samples": samples[:: max(1, len(samples) // 200)]}
 
 
 def atmosphere_request_maker(sizes=((128, 256), (256, 512), (384, 768), (512, 1024)),

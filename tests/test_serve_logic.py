@@ -36,6 +36,24 @@ class FakeBatch:
     def poll(self):
         return self.left.copy()
 
+    # the asynchronous protocol: a snapshot per ticket, reads filled at io_wait
+    def poll_begin(self):
+        self.snaps = getattr(self, "snaps", [])
+        self.snaps.append(self.left.copy())
+        self.log.append(("poll_begin", len(self.snaps) - 1))
+        return len(self.snaps) - 1
+
+    def poll_end(self, ticket):
+        self.log.append(("poll_end", ticket))
+        return self.snaps[ticket]
+
+    def state_async(self, slot, out):
+        out[...] = slot
+        return out
+
+    def io_wait(self):
+        pass
+
     def state(self, slot):
         return np.full(3, slot, dtype=float)
 
@@ -46,7 +64,7 @@ class FakeBatch:
 
 
 def prob(tag, cells):
-    return SimpleNamespace(tag=tag, interior=cells)
+    return SimpleNamespace(tag=tag, interior=cells, w=np.zeros(3))
 
 
 class Clock:
@@ -100,3 +118,28 @@ def test_poisson_stream_is_seeded_and_ordered():
     gaps = np.diff([0.0] + [r.arrival for r in a])
     assert np.all(gaps > 0) and 0.01 < gaps.mean() < 0.05
     assert len(poisson_stream(1000, 40.0, mk, duration=1.0)) < 80
+
+
+def test_next_chunk_is_queued_before_the_last_is_waited_for():
+    """With depth 2 the loop queues chunk k+1 (and its snapshot) before it
+    waits for snapshot k: the device always has a chunk to run while the host
+    retires and admits."""
+    reqs = [Request(0, prob("a", 4), 6, 0.0), Request(1, prob("b", 4), 20, 0.0)]
+    fb = FakeBatch(capacity=100)
+    ck = Clock()
+    Server(fb, chunk=2, depth=2).run(reqs, clock=ck, sleep=ck.sleep)
+    ev = [e for e in fb.log if e[0] in ("poll_begin", "poll_end")]
+    for k in range(len(fb.snaps) - 1):
+        assert ev.index(("poll_begin", k + 1)) < ev.index(("poll_end", k)), k
+    # a, done after 3 chunks, is retired from snapshot 2 while chunk 4 is queued
+    assert fb.log.index(("remove", 0)) > fb.log.index(("poll_begin", 3))
+
+
+def test_stop_after_reports_executed_work():
+    reqs = [Request(i, prob(i, 3), 50, 0.01 * i) for i in range(6)]
+    fb = FakeBatch(capacity=6)  # two at a time
+    ck = Clock()
+    st = Server(fb, chunk=5, depth=2).run(reqs, clock=ck, sleep=ck.sleep, stop_after=0.05)
+    assert st["completed"] < 6 and st["completed"] + st["unfinished_active"] + st["still_waiting"] == 6
+    done_work = sum(r.nsteps * 3 for r in reqs if r.done is not None)
+    assert st["cell_updates"] >= done_work
