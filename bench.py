@@ -658,19 +658,27 @@ def run_serving(a, ctx):
     import torch
 
     from smaug_b200 import PREC_MIXED, Batch
-    from smaug_b200.serve import Server, atmosphere_request_maker, poisson_stream
-    reqs = poisson_stream(a.serve_requests, 40.0, atmosphere_request_maker(), seed=777 + 1000 * ctx.rank,
-                          duration=a.serve_seconds)
+    from smaug_b200.serve import Server, atmosphere_request_maker, merge_stats, poisson_stream, shard
+    # one stream; with N GPUs each rank serves every N-th request as an
+    # independent replica (its own batch, no data-path collective)
+    stream = poisson_stream(a.serve_requests, 40.0, atmosphere_request_maker(), seed=777, duration=a.serve_seconds)
+    reqs = shard(stream, ctx.rank, ctx.world)
     free, _ = torch.cuda.mem_get_info()
     arena = min(int(free * 0.5), 32 << 30)
     b = Batch(2, precision=PREC_MIXED, arena_bytes=arena, max_sims=256, device=ctx.local)
     ctx.barrier()
-    st = Server(b, chunk=10, keep_results=False, depth=2).run(reqs, stop_after=a.serve_seconds)
+    srv = Server(b, chunk=10, keep_results=False, depth=2)
+    st = srv.run(reqs, stop_after=a.serve_seconds)
     b.close()
-    offered = sum(r.nsteps * r.prob.interior for r in reqs)
+    if ctx.dist is not None:  # the replicas' statistics, gathered once at the end
+        gathered = [None] * ctx.world
+        ctx.dist.all_gather_object(gathered, (st, srv.latencies))
+        st = dict(st, **merge_stats(gathered))
+    offered = sum(r.nsteps * r.prob.interior for r in stream)
     st.update({"arrival_rate_per_s": 40.0, "chunk_steps": 10, "pipeline_depth": 2, "arena_bytes": arena,
                "stream_seconds": a.serve_seconds,
-               "offered_cell_updates_per_s": offered / max(reqs[-1].arrival, 1e-9) if reqs else 0.0,
+               "offered_cell_updates_per_s": offered / max(stream[-1].arrival, 1e-9) if stream else 0.0,
+               "replicas": ctx.world,
                "workload": f"Poisson arrivals 40/s (seed 777), {a.serve_requests} requests or {a.serve_seconds:.0f} s, "
                            "of driven atmosphere x-z slices {128x256, 256x512, 384x768, 512x1024}, period "
                            "U[120,600] s, amplitude U[50,500] m/s, U[200,2000] steps, mixed precision; the server "

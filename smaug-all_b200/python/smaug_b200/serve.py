@@ -165,6 +165,7 @@ class Server:
         fin = [r for r in reqs if r.done is not None]
         lat = np.array([r.latency for r in fin])
         cell_updates = sum(steps_seen.get(r.rid, 0) * r.prob.interior for r in reqs)
+        self.latencies = [float(x) for x in lat]
         return {"requests": len(reqs), "completed": len(fin), "unfinished_active": len(active),
                 "still_waiting": len(queue) + (len(reqs) - i), "wall_s": wall, "chunks": chunks,
                 "max_active": max_active, "cell_updates": cell_updates,
@@ -173,6 +174,28 @@ class Server:
                 "p99_s": float(np.percentile(lat, 99)) if len(lat) else None,
                 "mean_s": float(lat.mean()) if len(lat) else None,
                 "queue_samples": samples[:: max(1, len(samples) // 200)]}
+
+
+def shard(requests, rank: int, world: int) -> list:
+    """The requests one of `world` replicas serves: every world-th request in
+    arrival order, starting at `rank` (each replica runs its own batch on its
+    own GPU; no data passes between them)."""
+    ordered = sorted(requests, key=lambda r: r.arrival)
+    return [r for k, r in enumerate(ordered) if k % world == rank]
+
+
+def merge_stats(per_rank: list) -> dict:
+    """Whole-stream statistics from the replicas' (stats, latencies) pairs:
+    requests and cell-updates add up, the wall time is the slowest
+    replica's, the percentiles are over every completed request."""
+    lat = np.concatenate([np.asarray(l, dtype=float) for _, l in per_rank]) if per_rank else np.zeros(0)
+    wall = max(st["wall_s"] for st, _ in per_rank)
+    cu = sum(st["cell_updates"] for st, _ in per_rank)
+    return {"replicas": len(per_rank), "requests": sum(st["requests"] for st, _ in per_rank),
+            "completed": int(len(lat)), "wall_s": wall, "cell_updates": cu,
+            "cell_updates_per_s": cu / wall if wall > 0 else 0.0,
+            "p50_s": float(np.percentile(lat, 50)) if len(lat) else None,
+            "p99_s": float(np.percentile(lat, 99)) if len(lat) else None}
 
 
 def atmosphere_request_maker(sizes=((128, 256), (256, 512), (384, 768), (512, 1024)),
@@ -191,4 +214,4 @@ def atmosphere_request_maker(sizes=((128, 256), (256, 512), (384, 768), (512, 10
     return make
 
 
-__all__ = ["Request", "Server", "poisson_stream", "atmosphere_request_maker", "PREC_MIXED"]
+__all__ = ["Request", "Server", "poisson_stream", "atmosphere_request_maker", "shard", "merge_stats", "PREC_MIXED"]
