@@ -70,12 +70,21 @@ class Server:
     free up (admissions run on their own stream and do not wait for the
     queued chunks either)."""
 
-    def __init__(self, batch, chunk: int = 8, keep_results: bool = True, depth: int = 2):
+    def __init__(self, batch, chunk: int = 8, keep_results: bool = True, depth: int = 2, time_chunks: bool = False):
         self.batch = batch
         self.chunk = chunk
         self.keep_results = keep_results
         self.depth = max(1, depth)
+        # CUDA events around every chunk on the batch's stream: the device's
+        # busy time while serving (needs torch and a batch with a stream)
+        self.time_chunks = time_chunks
         self._pool: dict = {}
+
+    def _chunk_events(self):
+        import torch
+        st = torch.cuda.ExternalStream(self.batch.stream)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        return st, e0, e1
 
     def _buffer(self, shape):
         free = self._pool.setdefault(shape, [])
@@ -105,6 +114,7 @@ class Server:
         inflight: deque = deque()  # (ticket, [(slot, rid)]) in queue order
         i, chunks, max_active = 0, 0, 0
         samples = []  # (t, waiting, active)
+        events = []   # (start, end) of every chunk on the device
         stopped = False
         while True:
             t = now()
@@ -125,7 +135,13 @@ class Server:
             max_active = max(max_active, len(active))
             samples.append((round(t, 3), len(queue), len(active)))
             if active and not stopped and len(inflight) < self.depth:
+                if self.time_chunks:
+                    st_, e0, e1 = self._chunk_events()
+                    e0.record(st_)
                 self.batch.step(self.chunk)
+                if self.time_chunks:
+                    e1.record(st_)
+                    events.append((e0, e1))
                 chunks += 1
                 inflight.append((self.batch.poll_begin(), [(s_, r_.rid) for s_, r_ in active.items()]))
                 if len(inflight) < self.depth:
@@ -166,7 +182,13 @@ class Server:
         lat = np.array([r.latency for r in fin])
         cell_updates = sum(steps_seen.get(r.rid, 0) * r.prob.interior for r in reqs)
         self.latencies = [float(x) for x in lat]
-        return {"requests": len(reqs), "completed": len(fin), "unfinished_active": len(active),
+        dev = {}
+        if events:
+            events[-1][1].synchronize()
+            busy = sum(a.elapsed_time(b) for a, b in events) / 1e3
+            span = events[0][0].elapsed_time(events[-1][1]) / 1e3
+            dev = {"gpu_busy_s": busy, "gpu_span_s": span, "gpu_busy_fraction": busy / span if span > 0 else 0.0}
+        return {**dev, "requests": len(reqs), "completed": len(fin), "unfinished_active": len(active),
                 "still_waiting": len(queue) + (len(reqs) - i), "wall_s": wall, "chunks": chunks,
                 "max_active": max_active, "cell_updates": cell_updates,
                 "cell_updates_per_s": cell_updates / wall if wall > 0 else 0.0,
