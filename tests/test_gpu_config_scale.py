@@ -27,10 +27,13 @@ Bars:
   viscous dt), dt within 1e-9;
 * mixed at a fixed dt (half the dt the rule reaches): 1e-5 per field, the
   north-star bar on the arithmetic itself;
-* mixed under the dt rule: dt within 2e-4 of the oracle's (its viscous limit
-  divides by a hyperviscosity coefficient formed from FP32 states), and 1e-4
-  per field -- a different dt moves the state by about that relative amount
-  times the state's change over the run.
+* mixed under the dt rule: dt within 2e-3 of the oracle's, and 1e-4 per field
+  -- a different dt moves the state by about that relative amount times the
+  state's change over the run.  The viscous limit divides by the largest
+  hyperviscosity coefficient, max|d3 q| / max|d1 q| with q formed from FP32
+  states; the third differences shrink as (k dx)^3 with resolution, so FP32
+  rounding of q weighs more on finer grids (8e-4 measured on the 256^2 vortex
+  after 10 steps, against 2e-5 on 48^2).
 """
 from __future__ import annotations
 
@@ -110,7 +113,7 @@ def test_production_kernel_vs_oracle_at_config_size(need_gpu, name, mode):
     e.close()
     tol = FP64_TOL if prec == PREC_FP64 else (MIXED_TOL if fixed else MIXED_DT_RULE_TOL)
     assert np.all(err <= tol), (name, mode, err)
-    assert abs(dt - dt_ref) <= (1e-9 if prec == PREC_FP64 else 2e-4) * dt_ref, (dt, dt_ref)
+    assert abs(dt - dt_ref) <= (1e-9 if prec == PREC_FP64 else 2e-3) * dt_ref, (dt, dt_ref)
 
 
 @pytest.mark.parametrize("mode", ["fp64-dt_rule", "mixed-fixed_dt"])
