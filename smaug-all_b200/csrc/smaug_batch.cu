@@ -72,7 +72,9 @@ size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
 size_t sim_footprint(const SimPlan &p) {
   const size_t N = (size_t)p.geo.N;
   size_t b = align256(sizeof(DevScalars));
-  b += 2 * align256(sizeof(double) * (size_t)(p.geo.n[0] + p.geo.n[1] + p.geo.n[2]));  // metric, driver
+  const size_t nl = (size_t)(p.geo.n[0] + p.geo.n[1] + p.geo.n[2]);
+  b += align256(2 * sizeof(double) * nl);  // metric lines and their reciprocals
+  b += align256(sizeof(double) * nl);      // driver lines
   b += align256(sizeof(double) * N);                  // dxlast
   b += align256(sizeof(double) * (size_t)p.NB * N);   // backgrounds
   b += align256(sizeof(double) * (size_t)p.NW * N);   // W[0]
@@ -471,8 +473,10 @@ int smaug_batch_add(smaug_batch *b, const smaug_params *prm, const double *delx,
   if (!p.rk4 || p.exact) return bfail(b, SMAUG_ERR_ARG, "batch simulations use rk4 = 1 and exact = 0");
   const long long N = p.geo.N;
   // one line per dim here; the metric itself is checked on the device below
-  std::vector<double> d1(p.geo.n[0] + p.geo.n[1] + p.geo.n[2]);
+  const size_t nl = (size_t)p.geo.n[0] + p.geo.n[1] + p.geo.n[2];
+  std::vector<double> d1(2 * nl);  // the lines, then their reciprocals
   metric_lines_host(p, delx, d1.data());
+  for (size_t i = 0; i < nl; ++i) d1[nl + i] = 1.0 / d1[i];
   BK(cudaSetDevice(b->device));
   // a slot and a block: first from what is free now, then, if removed
   // simulations still wait for their queued work, after waiting for it
@@ -511,8 +515,8 @@ int smaug_batch_add(smaug_batch *b, const smaug_params *prm, const double *delx,
   };
   DevScalars *sc = (DevScalars *)take(sizeof(DevScalars));
   double *dx1 = (double *)take(sizeof(double) * d1.size());
-  double *drv = (double *)take(sizeof(double) * d1.size());
-  std::vector<double> drv_host(d1.size());
+  double *drv = (double *)take(sizeof(double) * nl);
+  std::vector<double> drv_host(nl);
   driver_lines(p, prm, drv_host.data());
   double *dxlast = (double *)take(sizeof(double) * N);
   double *bg = (double *)take(sizeof(double) * p.NB * N);
@@ -530,6 +534,7 @@ int smaug_batch_add(smaug_batch *b, const smaug_params *prm, const double *delx,
   size_t o1 = 0;
   for (int d = 0; d < p.D; ++d) {
     p.geo.dx1[d] = dx1 + o1;
+    p.geo.rdx1[d] = dx1 + nl + o1;
     o1 += p.geo.n[d];
   }
   p.geo.dxlast = dxlast;

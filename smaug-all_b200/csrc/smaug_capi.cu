@@ -305,7 +305,7 @@ int smaug_create(const smaug_params *prm, int device, smaug_ctx **out) {
   if (r.mixed)
     for (auto &f : r.F) CK(cudaMalloc(&f, sizeof(float) * (size_t)r.geo.N * r.NW));
   CK(cudaMalloc(&r.bg, fsz * r.NB));
-  CK(cudaMalloc(&ctx->dx1, sizeof(double) * (r.geo.n[0] + r.geo.n[1] + r.geo.n[2])));
+  CK(cudaMalloc(&ctx->dx1, 2 * sizeof(double) * (r.geo.n[0] + r.geo.n[1] + r.geo.n[2])));  // lines, reciprocals
   CK(cudaMalloc(&ctx->dxlast, fsz));
   CK(cudaMalloc(&r.sc, sizeof(DevScalars)));
   CK(cudaMalloc(&r.inst, sizeof(BatchInst)));
@@ -359,13 +359,16 @@ int smaug_set_metric(smaug_ctx *ctx, const double *delx, size_t count) {
   CK(cudaSetDevice(ctx->device));
   // The stencils use delx at inner cells only, where the reference's metric
   // depends on that coordinate alone: keep one line per dim.
-  std::vector<double> d1(r.geo.n[0] + r.geo.n[1] + r.geo.n[2]);
+  const size_t nl = (size_t)r.geo.n[0] + r.geo.n[1] + r.geo.n[2];
+  std::vector<double> d1(2 * nl);  // the lines, then their reciprocals
   double minsq[3];
   if (const char *m = metric_host(r, delx, d1.data(), minsq)) return fail(ctx, SMAUG_ERR_ARG, m);
+  for (size_t i = 0; i < nl; ++i) d1[nl + i] = 1.0 / d1[i];
   CK(cudaMemcpyAsync(ctx->dx1, d1.data(), sizeof(double) * d1.size(), cudaMemcpyHostToDevice, r.stream));
   size_t off = 0;
   for (int d = 0; d < D; ++d) {
     r.geo.dx1[d] = ctx->dx1 + off;
+    r.geo.rdx1[d] = ctx->dx1 + nl + off;
     off += r.geo.n[d];
   }
   CK(cudaMemcpyAsync(ctx->dxlast, delx + (size_t)(D - 1) * N, sizeof(double) * N, cudaMemcpyHostToDevice,
@@ -653,7 +656,7 @@ int smaug_step_noalloc(const smaug_params *prm, const double *delx_dev, const do
   const size_t head = (sizeof(DevScalars) + 255) / 256 * 256 + (sizeof(BatchInst) + 255) / 256 * 256;
   const size_t lines = ((size_t)(r.geo.n[0] + r.geo.n[1] + r.geo.n[2]) * sizeof(double) + 255) / 256 * 256;
   const size_t field = ((size_t)r.NW * (size_t)N * sizeof(double) + 255) / 256 * 256;
-  const size_t need = head + 2 * lines + 3 * field;  // metric lines, driver lines, RK buffers
+  const size_t need = head + 3 * lines + 3 * field;  // metric lines and reciprocals, driver lines, RK buffers
   if (need > (size_t)SMAUG_NOALLOC_SCRATCH_BYTES) {
     char msg[160];
     std::snprintf(msg, sizeof(msg), "grid needs %zu bytes of scratch, above the %u-byte maximum of smaug_step_noalloc",
@@ -674,11 +677,13 @@ int smaug_step_noalloc(const smaug_params *prm, const double *delx_dev, const do
   double *dx1 = (double *)(s + head);
   r.W[0] = w_out_dev;
   r.bg = w_out_dev + (size_t)r.NW * N;
-  double *drv = (double *)(s + head + lines);
-  for (int k = 0; k < 3; ++k) r.W[1 + k] = (double *)(s + head + 2 * lines + k * field);
+  double *drv = (double *)(s + head + 2 * lines);
+  for (int k = 0; k < 3; ++k) r.W[1 + k] = (double *)(s + head + 3 * lines + k * field);
+  const size_t nl = (size_t)r.geo.n[0] + r.geo.n[1] + r.geo.n[2];  // metric_kernel writes the reciprocals after the lines
   size_t off = 0;
   for (int d = 0; d < r.D; ++d) {
     r.geo.dx1[d] = dx1 + off;
+    r.geo.rdx1[d] = dx1 + nl + off;
     off += r.geo.n[d];
   }
   r.geo.dxlast = delx_dev + (size_t)(r.D - 1) * N;

@@ -195,6 +195,12 @@ __device__ __forceinline__ void dt_update(DevScalars *sc, const Phys &p, int D) 
   }
   if (!isfinite(sc->dt) || sc->dt <= 0.0) sc->status = SMAUG_ERR_NONFINITE;
   for (int s = 1; s < 5; ++s) sc->red[s] = sc->floor;
+  // the RK stage sizes, divided as the oracle divides (dt/2, dt/2, dt, dt/6)
+  sc->hst[0] = 0.0;
+  sc->hst[1] = sc->dt / 2.0;
+  sc->hst[2] = sc->dt / 2.0;
+  sc->hst[3] = sc->dt / 1.0;
+  sc->hst[4] = sc->dt / 6.0;
 }
 
 // End of step: running maximum of the hyperviscosity (the reference's reset
@@ -326,14 +332,20 @@ __global__ void metric_kernel(const double *delx, Geo g, int D, double *dx1, Dev
   const long long tid = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   const long long nthr = (long long)gridDim.x * blockDim.x;
   long long off = 0;
+  const long long nl = (long long)g.n[0] + g.n[1] + g.n[2];  // the reciprocals follow the lines
   for (int d = 0; d < D && dx1; ++d) {
     for (long long x = tid; x < g.n[d]; x += nthr) {
       int c[3] = {2, 2, D == 3 ? 2 : 0};
       c[d] = (int)x;
-      dx1[off + x] = delx[(long long)d * g.N + c[0] + c[1] * g.st[1] + c[2] * g.st[2]];
+      const double v = delx[(long long)d * g.N + c[0] + c[1] * g.st[1] + c[2] * g.st[2]];
+      dx1[off + x] = v;
+      dx1[nl + off + x] = 1.0 / v;
     }
     off += g.n[d];
   }
+  // minimum of delx_d^2 over the first K cells: per thread, then per warp,
+  // then one atomic per warp (positive doubles order as their bit patterns)
+  unsigned long long mn[3] = {~0ull, ~0ull, ~0ull};
   const unsigned n0 = (unsigned)g.n[0], n1 = (unsigned)g.n[1];
   for (long long j = tid; j < g.N; j += nthr) {
     unsigned q = (unsigned)j;
@@ -354,8 +366,19 @@ __global__ void metric_kernel(const double *delx, Geo g, int D, double *dx1, Dev
         if (v != delx[(long long)d * g.N + cl[0] + cl[1] * g.st[1] + cl[2] * g.st[2]])
           atomicExch(&sc->status, (int)SMAUG_ERR_ARG);
       }
-      if (j < g.K) atomicMin((unsigned long long *)&sc->minsq[d], (unsigned long long)__double_as_longlong(v * v));
+      if (j < g.K) {
+        const unsigned long long b = (unsigned long long)__double_as_longlong(v * v);
+        if (b < mn[d]) mn[d] = b;
+      }
     }
+  }
+  for (int d = 0; d < D; ++d) {
+    unsigned long long m = mn[d];
+    for (int o = 16; o > 0; o >>= 1) {
+      const unsigned long long y = __shfl_xor_sync(0xffffffffu, m, o);
+      m = y < m ? y : m;
+    }
+    if ((threadIdx.x & 31) == 0 && m != ~0ull) atomicMin((unsigned long long *)&sc->minsq[d], m);
   }
 }
 

@@ -39,6 +39,7 @@ struct DevScalars {
   int go;         // batch only: this simulation takes the current step
   int bg_live;    // set on load: the state has a nonzero energy background (e_b, B_b)
   double t;       // simulation time at the start of the current step (driver)
+  double hst[5];  // RK stage sizes of the current step: [1..4] = dt/2, dt/2, dt, dt/6 (set with dt)
   Reduce red[5];  // [0] state at step start, [1..3] RK stage outputs, [4] state at step end
   // maxima over the ghost cells that keep their loaded values (fixed
   // boundaries): the stage kernels never rewrite those cells, so each step's
@@ -56,6 +57,7 @@ struct Geo {
   int has_const;              // some ghost cells keep their loaded values (a fixed dim)
   long long K;                // courant cells below K are excluded from the viscous-dt maximum
   const double *dx1[3];       // metric along d at inner cells (depends on c_d only)
+  const double *rdx1[3];      // its reciprocals 1 / dx1 (IEEE division, once per grid line)
   const double *dxlast;       // full per-cell metric of the last dim (courant reduction)
   const double *drvf[3];      // driver: Gaussian factor per cell index along each dim
 };
@@ -90,6 +92,7 @@ struct StageArgs {
   int kind;            // FP64: 0 plain, 3 = RK stage 3, 4 = RK stage 4; mixed: RK stage 1..4
   int red_in, red_out; // reduction slots: cmax of `in`, maxima of `out`
   double hdiv;         // h = dt / hdiv (dt/2, dt/2, dt, dt/6 as the oracle divides)
+  int hslot;           // > 0: h is sc->hst[hslot], the same division done once per step
   double tfrac;        // stage input time = t + tfrac * dt (0, 1/2, 1/2, 1; driver)
 };
 

@@ -553,7 +553,7 @@ __device__ __forceinline__ void tile_body(const StageArgs &a, const Geo &g, cons
   const long long idx = active ? gidx<D>(g, c) : 0;
   const CellT<D, T> C{MIXED ? (const T *)(const void *)a.in32 : (const T *)(const void *)a.in, a.bg, g.N};
   const double dt = a.sc->dt;
-  const double h = dt / a.hdiv;
+  const double h = a.hslot > 0 ? a.sc->hst[a.hslot] : dt / a.hdiv;
   T cm[3] = {0, 0, 0};
 #pragma unroll
   for (int d = 0; d < D; ++d) cm[d] = (T)red_get(a.sc->red[a.red_in], d);
@@ -561,7 +561,7 @@ __device__ __forceinline__ void tile_body(const StageArgs &a, const Geo &g, cons
   T idx1[3] = {0, 0, 0};
   if (active) {
 #pragma unroll
-    for (int d = 0; d < D; ++d) idx1[d] = (T)(1.0 / __ldg(g.dx1[d] + c[d]));
+    for (int d = 0; d < D; ++d) idx1[d] = (T)__ldg(g.rdx1[d] + c[d]);
   }
   T dL[NW];
 #pragma unroll

@@ -215,7 +215,7 @@ __device__ __forceinline__ void tile_body2(const StageArgs &a, const Geo &g, con
   const bool active = c[0] <= n0 - 3 && c[1] <= n1 - 3;
   const long long idx = active ? c[0] + (long long)c[1] * g.st[1] : 0;
   const CellT<2, T> C{MIXED ? (const T *)(const void *)a.in32 : (const T *)(const void *)a.in, a.bg, g.N};
-  const double h = a.sc->dt / a.hdiv;
+  const double h = a.hslot > 0 ? a.sc->hst[a.hslot] : a.sc->dt / a.hdiv;
   const T cm[2] = {(T)red_get(a.sc->red[a.red_in], 0), (T)red_get(a.sc->red[a.red_in], 1)};
   prefetch_epilogue_rows<T, TX, TY, NT>(a, g, p, ox, oy);
   if (nbx >= 0) prefetch_qbox_rows<T, TX, TY, NT>(a, g, p, nbx, nby);
@@ -309,7 +309,7 @@ __device__ __forceinline__ void tile_body2(const StageArgs &a, const Geo &g, con
   T numax = 0;
   if (active) {
     const int tx = c[0] - ox, ty = c[1] - oy;
-    const T idx1[2] = {(T)(1.0 / __ldg(g.dx1[0] + c[0])), (T)(1.0 / __ldg(g.dx1[1] + c[1]))};
+    const T idx1[2] = {(T)__ldg(g.rdx1[0] + c[0]), (T)__ldg(g.rdx1[1] + c[1])};
     const int r0 = (tx + 3) + B::QX * (ty + 3);
     // flux divergences: -(8 (F_+1 - F_-1) - (F_+2 - F_-2)) / (12 dx), the
     // fluxes of the neighbours (inside the grid: the cell is an inner cell)

@@ -88,8 +88,8 @@ def test_batch_footprint_and_argument_checks():
     p = problems.orszag_tang(30)
     N, NW, NB = p.ncells, 6, 4
     a = lambda x: (x + 255) // 256 * 256  # noqa: E731  (arena blocks are 256-byte aligned)
-    lines = a(8 * (p.n[0] + p.n[1] + 1))
-    base = 2 * lines + a(8 * N) + a(8 * NB * N) + a(8 * NW * N)  # metric and driver lines
+    nl = p.n[0] + p.n[1] + 1
+    base = a(16 * nl) + a(8 * nl) + a(8 * N) + a(8 * NB * N) + a(8 * NW * N)  # metric lines + reciprocals, driver
     fp64 = footprint(p, PREC_FP64)
     mixed = footprint(p, PREC_MIXED)
     # scalars block + metric and driver lines + dxlast + backgrounds + W0, then 3 FP64 or 5 FP32 buffers
