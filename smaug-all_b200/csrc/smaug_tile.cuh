@@ -114,7 +114,7 @@ __device__ __forceinline__ void fluxes_fast(const CellT<D, T> &c, long long i, i
   using L = Lay<D>;
   const T rho = c.v(L::RHO, i);
   const double rt = (double)rho + c.vd(L::RHOB, i);
-  const double irtd = 1.0 / rt;
+  const double irtd = __drcp_rn(rt);
   const T irt = (T)irtd;
   T m[D], b[D], bb[D];
 #pragma unroll
@@ -157,7 +157,7 @@ template <int D, typename T>
 __device__ __forceinline__ void q_all(const CellT<D, T> &c, long long i, int d, T *q) {
   using L = Lay<D>;
   const T rho = c.v(L::RHO, i);
-  const double irtd = 1.0 / ((double)rho + c.vd(L::RHOB, i));
+  const double irtd = __drcp_rn((double)rho + c.vd(L::RHOB, i));
   const T irt = (T)irtd;
   double b2 = 0, m2 = 0;
   q[0] = rho;
@@ -610,7 +610,7 @@ __device__ __forceinline__ void tile_body(const StageArgs &a, const Geo &g, cons
 
   // ------------------------------------------------ gravity
   if (active && p.has_grav) {
-    const T rho = C.v(L::RHO, idx), irt = (T)(1.0 / ((double)rho + C.vd(L::RHOB, idx)));
+    const T rho = C.v(L::RHO, idx), irt = (T)__drcp_rn((double)rho + C.vd(L::RHOB, idx));
 #pragma unroll
     for (int k = 0; k < D; ++k) {
       dL[L::M0 + k] += (T)p.g[k] * rho;

@@ -39,7 +39,7 @@ __device__ __forceinline__ void q_cell(const CellT<2, T> &c, long long i, double
   using L = Lay<2>;
   const T rho = c.v(L::RHO, i);
   const double rhob = c.vd(L::RHOB, i);
-  const double irtd = 1.0 / ((double)rho + rhob);
+  const double irtd = __drcp_rn((double)rho + rhob);
   const T irt = (T)irtd;
   const T m0 = c.v(L::M0, i), m1 = c.v(L::M0 + 1, i), b0 = c.v(L::B0, i), b1 = c.v(L::B0 + 1, i);
   const T e = c.v(L::EN, i);
@@ -336,7 +336,7 @@ __device__ __forceinline__ void tile_body2(const StageArgs &a, const Geo &g, con
     div_terms(std::integral_constant<int, 1>{});
     // gravity
     if (p.has_grav) {
-      const T rho = C.v(L::RHO, idx), irt = (T)(1.0 / ((double)rho + C.vd(L::RHOB, idx)));
+      const T rho = C.v(L::RHO, idx), irt = (T)__drcp_rn((double)rho + C.vd(L::RHOB, idx));
 #pragma unroll
       for (int k = 0; k < 2; ++k) {
         dL[L::M0 + k] += (T)p.g[k] * rho;
