@@ -24,6 +24,7 @@
 #include <type_traits>
 
 #include "smaug_tile.cuh"
+#include "smaug_pair.cuh"
 
 namespace SMAUG_NS {
 using namespace smaug;
@@ -94,6 +95,35 @@ __device__ __forceinline__ void flux_q(const T *Q, int r, bool bgb, T *F) {
   F[3] = vfma(vd, (e + eb) + pt, -vfma(bdt, bv, bd * bbv));
   const T bf = dir == 0 ? b1 : b0, bbf = dir == 0 ? bb1 : bb0, vf = dir == 0 ? v1 : v0;
   F[4] = vfma(vd, bf + bbf, -(bdt * vf));
+}
+
+// flux_q at two q-box cells at once (FP32 only): lane lo at cell ra, lane hi
+// at cell rb, each lane the same operations in the same order as flux_q, so
+// the same bits.
+template <int dir, int QN>
+__device__ __forceinline__ void flux_q2(const float *Q, int ra, int rb, bool bgb, f2 *F) {
+  auto ld = [&](int slot) { return f2_make(Q[slot * QN + ra], Q[slot * QN + rb]); };
+  const f2 v0 = ld(2), v1 = ld(3), b0 = ld(4), b1 = ld(5);
+  const f2 m0 = ld(7), m1 = ld(8), e = ld(9), pt = ld(10);
+  f2 bb0 = f2_splat(0.0f), bb1 = bb0, eb = bb0;
+  if (bgb) {
+    bb0 = ld(11);
+    bb1 = ld(12);
+    eb = ld(13);
+  }
+  const f2 vd = dir == 0 ? v0 : v1, bd = dir == 0 ? b0 : b1, bbd = dir == 0 ? bb0 : bb1;
+  const f2 bdt = bd + bbd;
+  F[0] = dir == 0 ? m0 : m1;
+  F[1] = pfma(vd, m0, pneg(pfma(b0, bdt, bb0 * bd)));
+  F[2] = pfma(vd, m1, pneg(pfma(b1, bdt, bb1 * bd)));
+  if (dir == 0)
+    F[1] = F[1] + pt;
+  else
+    F[2] = F[2] + pt;
+  const f2 bv = pfma(b1, v1, b0 * v0), bbv = pfma(bb1, v1, bb0 * v0);
+  F[3] = pfma(vd, (e + eb) + pt, pneg(pfma(bdt, bv, bd * bbv)));
+  const f2 bf = dir == 0 ? b1 : b0, bbf = dir == 0 ? bb1 : bb0, vf = dir == 0 ? v1 : v0;
+  F[4] = pfma(vd, bf + bbf, pneg(bdt * vf));
 }
 
 // Box sizes of the three-phase body for a TX x TY tile.
@@ -243,19 +273,20 @@ __device__ __forceinline__ void tile_body2(const StageArgs &a, const Geo &g, con
   __syncthreads();
 
   // ------------------------------------------------ phase B: face ratios along x and y
-  // One work unit: SEG consecutive faces along d of one q slot on one line of
-  // the tile.  The line's q values are read once, each first difference
+  // One work unit: SEG consecutive faces along d (RUN, or the whole line if
+  // it is shorter) of one q slot on one line of the tile.  The line's q values are read once, each first difference
   // |q_j+1 - q_j| and third difference |3 (q_j+1 - q_j) - (q_j+2 - q_j-1)| is
   // formed once, and each face takes the max of the five first and the three
   // third differences around it.  The last run of a line is shifted back to
   // end at the line's last face (faces it shares with the run before are
   // written twice, with the same value).
-  constexpr int SEG = 5;
-  constexpr int NS0 = (TX + 1 + SEG - 1) / SEG, NS1 = (TY + 1 + SEG - 1) / SEG;
+  constexpr int RUN = 9;  // faces per run, at most a line's
+  constexpr int SEG0 = RUN < TX + 1 ? RUN : TX + 1, SEG1 = RUN < TY + 1 ? RUN : TY + 1;
+  constexpr int NS0 = (TX + 1 + SEG0 - 1) / SEG0, NS1 = (TY + 1 + SEG1 - 1) / SEG1;
   constexpr int NU0 = 5 * (TY + 2) * NS0, NU1 = 5 * (TX + 2) * NS1;
-  static_assert(SEG <= TX + 1 && SEG <= TY + 1, "a run must fit in a line");
   auto face_run = [=](auto dc, int u) {
     constexpr int d = decltype(dc)::value;
+    constexpr int SEG = d == 0 ? SEG0 : SEG1;
     constexpr int NL = d == 0 ? TX : TY;  // faces of a line: -1 .. NL-1 (tile-relative left cell)
     int line, s, k;  // line: the row (d = 0) or column (d = 1) + 1, tile-relative
     if (d == 0) {
@@ -319,6 +350,19 @@ __device__ __forceinline__ void tile_body2(const StageArgs &a, const Geo &g, con
       if (z4(g, c, dir)) return;
       constexpr int sd = dir == 0 ? 1 : B::QX;
       const T w12 = idx1[dir] * (T)(1.0 / 12.0);
+      if constexpr (MIXED) {
+        // lanes: the +1 / -1 neighbour (lo) and the +2 / -2 one (hi)
+        f2 Fp[5], Fm[5];
+        flux_q2<dir, B::QN>((const float *)Q, r0 + sd, r0 + 2 * sd, p.has_bgb, Fp);
+        flux_q2<dir, B::QN>((const float *)Q, r0 - sd, r0 - 2 * sd, p.has_bgb, Fm);
+#pragma unroll
+        for (int k = 0; k < 5; ++k) {
+          const int f = k < 4 ? k : L::B0 + 1 - dir;
+          const f2 dd = Fp[k] - Fm[k];
+          dL[f] = vfma(-vfma((T)8, (T)f2_lo(dd), -(T)f2_hi(dd)), w12, dL[f]);
+        }
+        return;
+      }
       T Fp[5], Fm[5], d1[5];
       flux_q<dir, B::QN>(Q, r0 + sd, p.has_bgb, Fp);
       flux_q<dir, B::QN>(Q, r0 - sd, p.has_bgb, Fm);
