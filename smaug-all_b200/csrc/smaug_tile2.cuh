@@ -3,7 +3,7 @@
 // Same operator as tile_body (smaug_tile.cuh), reorganised for 2-D so that a
 // tile needs two block barriers instead of ten and reads the state from
 // global memory once per cell of the tile +-3:
-//   phase A  the q slots of every cell of the tile +-3 (q_cell: the six
+//   phase A  the q slots of every cell of the tile +-3 (q_from: the six
 //            hyperviscosity inputs rho, e_int, v_x, v_y, B_x, B_y, and what
 //            the fluxes and the momentum terms need at the neighbours);
 //   phase B  one loop over runs of cell faces of both dimensions: the ratio
@@ -35,16 +35,35 @@ using namespace smaug;
 // What the fluxes read beyond those: 9 e, 10 the total pressure p_T (formed
 // in FP64, as the reference's pressure recovery), and with an energy
 // background (bgb) 11 B_b,x, 12 B_b,y, 13 e_b (not written without one).
+// The raw values of one cell that its q slots are formed from (loaded
+// first, so that a thread's loads for all its q cells are in flight together).
 template <typename T>
-__device__ __forceinline__ void q_cell(const CellT<2, T> &c, long long i, double gam, bool bgb, T *q) {
+struct QRaw {
+  T rho, m0, m1, b0, b1, e, bb0, bb1, eb;
+  double rhob;
+};
+
+template <typename T>
+__device__ __forceinline__ void q_load(const CellT<2, T> &c, long long i, bool bgb, QRaw<T> &r) {
   using L = Lay<2>;
-  const T rho = c.v(L::RHO, i);
-  const double rhob = c.vd(L::RHOB, i);
+  r.rho = c.v(L::RHO, i);
+  r.rhob = c.vd(L::RHOB, i);
+  r.m0 = c.v(L::M0, i);
+  r.m1 = c.v(L::M0 + 1, i);
+  r.b0 = c.v(L::B0, i);
+  r.b1 = c.v(L::B0 + 1, i);
+  r.e = c.v(L::EN, i);
+  r.bb0 = bgb ? c.v(L::BB0, i) : T(0);
+  r.bb1 = bgb ? c.v(L::BB0 + 1, i) : T(0);
+  r.eb = bgb ? c.v(L::EB, i) : T(0);
+}
+
+template <typename T>
+__device__ __forceinline__ void q_from(const QRaw<T> &r, double gam, T *q) {
+  const T rho = r.rho, m0 = r.m0, m1 = r.m1, b0 = r.b0, b1 = r.b1, e = r.e, bb0 = r.bb0, bb1 = r.bb1;
+  const double rhob = r.rhob;
   const double irtd = __drcp_rn((double)rho + rhob);
   const T irt = (T)irtd;
-  const T m0 = c.v(L::M0, i), m1 = c.v(L::M0 + 1, i), b0 = c.v(L::B0, i), b1 = c.v(L::B0 + 1, i);
-  const T e = c.v(L::EN, i);
-  const T bb0 = bgb ? c.v(L::BB0, i) : T(0), bb1 = bgb ? c.v(L::BB0 + 1, i) : T(0);
   const double b2 = (double)b0 * (double)b0 + (double)b1 * (double)b1;
   const double m2 = (double)m0 * (double)m0 + (double)m1 * (double)m1;
   const double bbb = (double)b0 * (double)bb0 + (double)b1 * (double)bb1;
@@ -61,7 +80,7 @@ __device__ __forceinline__ void q_cell(const CellT<2, T> &c, long long i, double
   q[10] = (T)((gam - 1.0) * ((double)e - 0.5 * m2 * irtd) - (gam - 2.0) * (bbb + 0.5 * b2));
   q[11] = bb0;
   q[12] = bb1;
-  q[13] = bgb ? c.v(L::EB, i) : T(0);
+  q[13] = r.eb;
 }
 
 // The fluxes along dir at the q-box cell r, from its q slots (the physical
@@ -130,7 +149,7 @@ __device__ __forceinline__ void flux_q2(const float *Q, int ra, int rb, bool bgb
 template <typename S>
 struct Box2 {
   static constexpr int TX = S::TX, TY = S::TY;
-  static constexpr int NQS = 14;                        // q slots per cell (q_cell)
+  static constexpr int NQS = 14;                        // q slots per cell (q_from)
   static constexpr int QX = TX + 6, QN = QX * (TY + 6);  // q: tile +-3
   // face ratios along x: faces x+1/2 for x in [-1, TX), rows tile +-1
   static constexpr int V0X = TX + 1, V0N = (TX + 1) * (TY + 2);
@@ -190,7 +209,7 @@ __device__ __forceinline__ void prefetch_epilogue_rows(const StageArgs &a, const
 
 // The q box of tile (nbx, nby) of the same simulation (the block's next work
 // item), prefetched toward L2: the stage input's fields and the backgrounds that
-// q_cell reads, one prefetch per line of each row segment of the box, clamped to
+// q_load reads, one prefetch per line of each row segment of the box, clamped to
 // the grid.
 template <typename T, int TX, int TY, int NT>
 __device__ __forceinline__ void prefetch_qbox_rows(const StageArgs &a, const Geo &g, const Phys &p, int nbx,
@@ -251,31 +270,42 @@ __device__ __forceinline__ void tile_body2(const StageArgs &a, const Geo &g, con
   if (nbx >= 0) prefetch_qbox_rows<T, TX, TY, NT>(a, g, p, nbx, nby);
 
   // ------------------------------------------------ phase A: q on the tile +-3
-  for (int rr = t; rr < B::QN; rr += NT) {
-    int cx = ox - 3 + rr % B::QX, cy = oy - 3 + rr / B::QX;
-    T q[B::NQS];
-    const bool inx = cx >= 0 && cx < n0, iny = cy >= 0 && cy < n1;
-    // pads of the padded copies: right 0, left q(5); corners never read
-    // (slots 6..13 are read at the tile +-2 along one dimension only, always
-    // inside the grid)
-    if ((!inx && !iny) || cx >= n0 || cy >= n1) {
+  // A fixed number of q cells per thread (the loop unrolled, so that the
+  // compiler may issue a later cell's loads ahead of an earlier cell's math).
+  {
+    constexpr int NA = (B::QN + NT - 1) / NT;
 #pragma unroll
-      for (int k = 0; k < B::NQS; ++k) q[k] = 0;
-    } else {
-      if (cx < 0) cx = 5;
-      if (cy < 0) cy = 5;
-      q_cell<T>(C, cx + (long long)cy * g.st[1], p.gamma, p.has_bgb, q);
+    for (int u = 0; u < NA; ++u) {
+      const int rr = t + u * NT;
+      if (rr >= B::QN) continue;
+      int cx = ox - 3 + rr % B::QX, cy = oy - 3 + rr / B::QX;
+      const bool inx = cx >= 0 && cx < n0, iny = cy >= 0 && cy < n1;
+      T q[B::NQS];
+      // pads of the padded copies: right 0, left q(5); corners never read
+      // (slots 6..13 are read at the tile +-2 along one dimension only,
+      // always inside the grid)
+      if ((!inx && !iny) || cx >= n0 || cy >= n1) {
+#pragma unroll
+        for (int k = 0; k < B::NQS; ++k) q[k] = 0;
+      } else {
+        if (cx < 0) cx = 5;
+        if (cy < 0) cy = 5;
+        QRaw<T> raw;
+        q_load<T>(C, cx + (long long)cy * g.st[1], p.has_bgb, raw);
+        q_from<T>(raw, p.gamma, q);
+      }
+#pragma unroll
+      for (int k = 0; k < B::NQS; ++k)
+        if (k < 11 || p.has_bgb) Q[k * B::QN + rr] = q[k];
     }
-#pragma unroll
-    for (int k = 0; k < B::NQS; ++k)
-      if (k < 11 || p.has_bgb) Q[k * B::QN + rr] = q[k];
   }
   __syncthreads();
 
   // ------------------------------------------------ phase B: face ratios along x and y
   // One work unit: SEG consecutive faces along d (RUN, or the whole line if
-  // it is shorter) of one q slot on one line of the tile.  The line's q values are read once, each first difference
-  // |q_j+1 - q_j| and third difference |3 (q_j+1 - q_j) - (q_j+2 - q_j-1)| is
+  // it is shorter) of one q slot on one line of the tile.  The line's q
+  // values are read once, each first difference |q_j+1 - q_j| and third
+  // difference |3 (q_j+1 - q_j) - (q_j+2 - q_j-1)| is
   // formed once, and each face takes the max of the five first and the three
   // third differences around it.  The last run of a line is shifted back to
   // end at the line's last face (faces it shares with the run before are
