@@ -422,10 +422,14 @@ def run_plain(probs, prec, ctx, steps, warmup):
     return {"value": ctx.world * cells * steps / (ms_max / 1e3), "ms_per_step": ms_max / steps}
 
 
+E2E_STEP_EVERY = 8  # admissions between the steps queued while the ensemble uploads
+
+
 def run_e2e_batched(probs, prec, ctx, steps):
     """End to end through the public batch API with host buffers: admit every
-    simulation from pinned host memory, advance `steps` steps, read every
-    result back into pinned host memory."""
+    simulation from pinned host memory, advance each by `steps` steps, read
+    every result back into pinned host memory; uploads, steps and reads
+    overlap as a serving loop overlaps them."""
     import numpy as np
     import torch
 
@@ -443,10 +447,43 @@ def run_e2e_batched(probs, prec, ctx, steps):
     torch.cuda.synchronize()
 
     def job():
-        slots = [b.add(p, steps, w=t.numpy(), delx=m.numpy()) for p, t, m in zip(probs, ins, mets)]
-        b.step(steps)
-        for sl, o in zip(slots, outs):
-            b.state(sl, out=o.numpy())
+        # Every member takes exactly `steps` steps (its budget at admission).
+        # A step is queued every E2E_STEP_EVERY admissions, so the members
+        # admitted so far run while the next ones upload; the members
+        # admitted first then finish up to `queued` steps before the last
+        # one, and are read back (read-back stream, pinned buffers) while the
+        # last steps run.
+        slots, queued = [], 0
+        for i, (p, t, m) in enumerate(zip(probs, ins, mets)):
+            slots.append(b.add(p, steps, w=t.numpy(), delx=m.numpy()))
+            if (i + 1) % E2E_STEP_EVERY == 0 and queued < steps:
+                b.step(1)
+                queued += 1
+        pending = list(range(len(slots)))
+
+        def read_finished(left):
+            for k in [k for k in pending if left[slots[k]] == 0]:
+                b.state_async(slots[k], outs[k].numpy())
+                pending.remove(k)
+
+        rest = steps
+        first = rest - queued  # no member finishes before these are done
+        if first:
+            b.step(first)
+        rest -= first
+        tickets = [b.poll_begin()]
+        while rest > 0:
+            n = min(2, rest)
+            b.step(n)
+            rest -= n
+            tickets.append(b.poll_begin())
+            if len(tickets) > 2:  # the older snapshot: read what had finished there
+                read_finished(b.poll_end(tickets.pop(0)))
+        for tk in tickets:
+            read_finished(b.poll_end(tk))
+        b.io_wait()
+        if pending:
+            raise RuntimeError(f"e2e: {len(pending)} simulations did not finish their steps")
 
     ms = event_ms(stream, job)
     b.close()
