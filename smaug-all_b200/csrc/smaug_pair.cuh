@@ -21,13 +21,13 @@ __device__ __forceinline__ f2 f2_make(float lo, float hi) {
 }
 __device__ __forceinline__ f2 f2_splat(float a) { return f2_make(a, a); }
 __device__ __forceinline__ float f2_lo(f2 x) {
-  float lo, hi;
-  asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(x.r));
+  float lo;
+  asm("{\n\t.reg .f32 h;\n\tmov.b64 {%0, h}, %1;\n\t}" : "=f"(lo) : "l"(x.r));
   return lo;
 }
 __device__ __forceinline__ float f2_hi(f2 x) {
-  float lo, hi;
-  asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(x.r));
+  float hi;
+  asm("{\n\t.reg .f32 l;\n\tmov.b64 {l, %0}, %1;\n\t}" : "=f"(hi) : "l"(x.r));
   return hi;
 }
 __device__ __forceinline__ f2 operator+(f2 a, f2 b) {
