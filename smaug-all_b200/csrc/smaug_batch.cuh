@@ -29,7 +29,7 @@ struct WorkItem {
 // allocation is made for) the stage kernel is built for; the autotuner picks
 // one.  Variant 0 is the single-simulation default.
 constexpr int kBatchVariants2 = 11;
-constexpr int kBatchVariants3 = 6;
+constexpr int kBatchVariants3 = 8;
 struct BatchVariant {
   int t[3];
   int min_blocks;
@@ -56,6 +56,8 @@ __host__ __device__ inline BatchVariant batch_variant(int D, int v) {
     case 3: return {{8, 8, 4}, 3};
     case 4: return {{16, 8, 2}, 3};
     case 5: return {{8, 8, 4}, 4};
+    case 6: return {{8, 8, 8}, 2};
+    case 7: return {{16, 8, 4}, 2};
     default: return {{8, 8, 4}, 2};
   }
 }
@@ -66,7 +68,7 @@ __host__ __device__ inline BatchVariant batch_variant(int D, int v) {
 // and a single-simulation context on the same variant give the same bits.
 __host__ __device__ inline int batch_default_variant(int D, bool mixed) {
   if (D == 2) return mixed ? 8 : 0;
-  return mixed ? 5 : 0;
+  return mixed ? 6 : 0;
 }
 
 __host__ __device__ inline void batch_tile_shape(int D, int v, int *t) {

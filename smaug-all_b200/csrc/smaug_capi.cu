@@ -43,6 +43,7 @@ struct Run : SimPlan {
   BatchInst *inst = nullptr;
   BatchInst h_inst{};
   int ntiles = 0;
+  int grid = 0;  // persistent grid of the batch stage kernel (blocks), at most ntiles
   int cur = 0;
   long long launches = 0;
   // optional per-stage timing
@@ -118,7 +119,7 @@ void launch_stage(Run &r, const StageArgs &a) {
 void launch_rk_stage(Run &r, int k) {
   timed_launch(r, [&] {
     smaug_batchk::launch_batch_stage(r.D, r.mixed, batch_default_variant(r.D, r.mixed), r.inst, nullptr, r.ntiles, k,
-                                     r.ntiles, r.stream);
+                                     r.grid, r.stream);
   });
   // its ghost pass: the ghost chunks of this simulation
   const int nch = (int)((ghost_cells(r.geo, r.D) + 255) / 256);
@@ -146,6 +147,12 @@ cudaError_t run_upload_inst(Run &r) {
     I.tiles[d] = d < r.D ? (r.geo.n[d] - 4 + t[d] - 1) / t[d] : 1;
     r.ntiles *= I.tiles[d];
   }
+  // a persistent grid, as a batch runs it: resident blocks on every SM, each
+  // looping over tiles and keeping its maxima across them
+  int dev = 0, sms = 148;
+  if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const int occ = std::max(1, smaug_batchk::batch_stage_occupancy(r.D, r.mixed, batch_default_variant(r.D, r.mixed)));
+  r.grid = std::min(r.ntiles, occ * sms);
   return cudaMemcpyAsync(r.inst, &I, sizeof(BatchInst), cudaMemcpyHostToDevice, r.stream);
 }
 
