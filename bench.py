@@ -425,6 +425,48 @@ def run_plain(probs, prec, ctx, steps, warmup):
 E2E_STEP_EVERY = 8  # admissions between the steps queued while the ensemble uploads
 
 
+def e2e_pipeline(b, probs, ws, mets, outs, steps: int):
+    """Admit every simulation (state ws[i], metric mets[i]) into batch b,
+    advance each by exactly `steps` steps (its budget at admission) and read
+    each state into outs[i].  A step is queued every E2E_STEP_EVERY
+    admissions, so the members admitted so far run while the next ones
+    upload; the members admitted first then finish up to `queued` steps
+    before the last one, and are read back (read-back stream, poll
+    snapshots) while the last steps run."""
+    slots, queued = [], 0
+    for i, (p, w, m) in enumerate(zip(probs, ws, mets)):
+        slots.append(b.add(p, steps, w=w, delx=m))
+        if (i + 1) % E2E_STEP_EVERY == 0 and queued < steps:
+            b.step(1)
+            queued += 1
+    pending = list(range(len(slots)))
+
+    def read_finished(left):
+        for k in [k for k in pending if left[slots[k]] == 0]:
+            b.state_async(slots[k], outs[k])
+            pending.remove(k)
+
+    rest = steps
+    first = rest - queued  # no member finishes before these are done
+    if first:
+        b.step(first)
+    rest -= first
+    tickets = [b.poll_begin()]
+    while rest > 0:
+        n = min(2, rest)
+        b.step(n)
+        rest -= n
+        tickets.append(b.poll_begin())
+        if len(tickets) > 2:  # the older snapshot: read what had finished there
+            read_finished(b.poll_end(tickets.pop(0)))
+    for tk in tickets:
+        read_finished(b.poll_end(tk))
+    b.io_wait()
+    if pending:
+        raise RuntimeError(f"e2e: {len(pending)} simulations did not finish their steps")
+    return slots
+
+
 def run_e2e_batched(probs, prec, ctx, steps):
     """End to end through the public batch API with host buffers: admit every
     simulation from pinned host memory, advance each by `steps` steps, read
@@ -447,43 +489,8 @@ def run_e2e_batched(probs, prec, ctx, steps):
     torch.cuda.synchronize()
 
     def job():
-        # Every member takes exactly `steps` steps (its budget at admission).
-        # A step is queued every E2E_STEP_EVERY admissions, so the members
-        # admitted so far run while the next ones upload; the members
-        # admitted first then finish up to `queued` steps before the last
-        # one, and are read back (read-back stream, pinned buffers) while the
-        # last steps run.
-        slots, queued = [], 0
-        for i, (p, t, m) in enumerate(zip(probs, ins, mets)):
-            slots.append(b.add(p, steps, w=t.numpy(), delx=m.numpy()))
-            if (i + 1) % E2E_STEP_EVERY == 0 and queued < steps:
-                b.step(1)
-                queued += 1
-        pending = list(range(len(slots)))
-
-        def read_finished(left):
-            for k in [k for k in pending if left[slots[k]] == 0]:
-                b.state_async(slots[k], outs[k].numpy())
-                pending.remove(k)
-
-        rest = steps
-        first = rest - queued  # no member finishes before these are done
-        if first:
-            b.step(first)
-        rest -= first
-        tickets = [b.poll_begin()]
-        while rest > 0:
-            n = min(2, rest)
-            b.step(n)
-            rest -= n
-            tickets.append(b.poll_begin())
-            if len(tickets) > 2:  # the older snapshot: read what had finished there
-                read_finished(b.poll_end(tickets.pop(0)))
-        for tk in tickets:
-            read_finished(b.poll_end(tk))
-        b.io_wait()
-        if pending:
-            raise RuntimeError(f"e2e: {len(pending)} simulations did not finish their steps")
+        e2e_pipeline(b, probs, [t.numpy() for t in ins], [m.numpy() for m in mets], [o.numpy() for o in outs],
+                     steps)
 
     ms = event_ms(stream, job)
     b.close()
