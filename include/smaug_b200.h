@@ -328,7 +328,8 @@ int smaug_batch_get_scalars(smaug_batch *b, int slot, double out[8]);
 /*
  * Autotuner: times RK stage 1 of the current simulations with every tile
  * shape the stage kernel is built for (reps launches each) and keeps the
- * fastest.  ms_out (nms entries, may be NULL) receives the per-shape times.
+ * fastest.  ms_out (nms entries, may be NULL) receives the per-shape times;
+ * -1 for a shape that cannot be resident on the device (not timed, never chosen).
  */
 int smaug_batch_tune(smaug_batch *b, int reps, int *variant_out, double *ms_out, int nms);
 int smaug_batch_set_variant(smaug_batch *b, int variant);

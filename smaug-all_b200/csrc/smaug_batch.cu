@@ -820,6 +820,13 @@ int smaug_batch_tune(smaug_batch *b, int reps, int *variant_out, double *ms_out,
   int best = b->variant;
   float best_ms = 1e30f;
   for (int v = 0; v < nv; ++v) {
+    // a shape that cannot be resident on this device (its shared memory or
+    // registers) is not timed: ms -1
+    if (smaug_batchk::batch_stage_occupancy(b->D, b->mixed, v) <= 0) {
+      (void)cudaGetLastError();
+      if (ms_out && v < nms) ms_out[v] = -1.0;
+      continue;
+    }
     b->variant = v;
     int rc = rebuild(b);
     if (rc != SMAUG_OK) return rc;
@@ -831,6 +838,12 @@ int smaug_batch_tune(smaug_batch *b, int reps, int *variant_out, double *ms_out,
       smaug_batchk::launch_batch_stage(b->D, b->mixed, v, b->d_tab, b->d_work, b->nwork, 1, b->grid, b->stream);
     BK(cudaEventRecord(e1, b->stream));
     BK(cudaEventSynchronize(e1));
+    // a launch that the device refused (a configuration error, reported
+    // synchronously) has timed nothing
+    if (cudaGetLastError() != cudaSuccess) {
+      if (ms_out && v < nms) ms_out[v] = -1.0;
+      continue;
+    }
     float ms = 0.f;
     BK(cudaEventElapsedTime(&ms, e0, e1));
     ms /= reps;
@@ -853,6 +866,11 @@ int smaug_batch_set_variant(smaug_batch *b, int variant) {
   if (!b) return SMAUG_ERR_ARG;
   const int nv = b->D == 2 ? kBatchVariants2 : kBatchVariants3;
   if (variant < 0 || variant >= nv) return bfail(b, SMAUG_ERR_ARG, "no such tile variant");
+  BK(cudaSetDevice(b->device));
+  if (smaug_batchk::batch_stage_occupancy(b->D, b->mixed, variant) <= 0) {
+    (void)cudaGetLastError();
+    return bfail(b, SMAUG_ERR_ARG, "tile variant cannot be resident on this device");
+  }
   b->variant = variant;
   b->dirty = true;
   return SMAUG_OK;
