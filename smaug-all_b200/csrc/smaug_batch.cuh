@@ -29,7 +29,7 @@ struct WorkItem {
 // allocation is made for) the stage kernel is built for; the autotuner picks
 // one.  Variant 0 is the single-simulation default.
 constexpr int kBatchVariants2 = 11;
-constexpr int kBatchVariants3 = 8;
+constexpr int kBatchVariants3 = 10;
 struct BatchVariant {
   int t[3];
   int min_blocks;
@@ -58,6 +58,8 @@ __host__ __device__ inline BatchVariant batch_variant(int D, int v) {
     case 5: return {{8, 8, 4}, 4};
     case 6: return {{8, 8, 8}, 2};
     case 7: return {{16, 8, 4}, 2};
+    case 8: return {{8, 8, 8}, 1};
+    case 9: return {{16, 8, 4}, 1};
     default: return {{8, 8, 4}, 2};
   }
 }
@@ -68,7 +70,7 @@ __host__ __device__ inline BatchVariant batch_variant(int D, int v) {
 // and a single-simulation context on the same variant give the same bits.
 __host__ __device__ inline int batch_default_variant(int D, bool mixed) {
   if (D == 2) return mixed ? 8 : 0;
-  return mixed ? 6 : 0;
+  return mixed ? 6 : 9;
 }
 
 __host__ __device__ inline void batch_tile_shape(int D, int v, int *t) {

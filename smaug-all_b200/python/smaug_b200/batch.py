@@ -143,7 +143,7 @@ class Batch:
         v = ctypes.c_int(-1)
         ms = (ctypes.c_double * 16)()
         self._check(self.lib.smaug_batch_tune(self.h, reps, ctypes.byref(v), ms, 16), "smaug_batch_tune")
-        nv = 11 if self.ndim == 2 else 8
+        nv = 11 if self.ndim == 2 else 10
         return v.value, list(ms[:nv])
 
     def set_variant(self, v: int):

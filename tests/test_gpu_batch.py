@@ -65,7 +65,7 @@ def test_batch_3d(need_gpu):
     b = Batch(3, precision=PREC_MIXED, arena_bytes=256 << 20, max_sims=4)
     slots = [b.add(p, 4) for p in probs]
     v, ms = b.tune(reps=2)
-    assert 0 <= v < 8 and len(ms) == 8 and all(m > 0 for m in ms)
+    assert 0 <= v < 10 and len(ms) == 10 and all(m > 0 for m in ms)
     b.step(4)
     for p, s in zip(probs, slots):
         assert np.array_equal(b.state(s), alone(p, 4, PREC_MIXED)[0])
@@ -73,11 +73,11 @@ def test_batch_3d(need_gpu):
 
 @pytest.mark.parametrize("precision", [PREC_MIXED, PREC_FP64])
 def test_batch_3d_tile_shapes_are_identical(need_gpu, precision):
-    """Every 3-D tile shape (256- and 512-thread tiles, ragged grids) gives
-    the bits of the simulation run alone."""
+    """Every 3-D tile shape (256- and 512-thread tiles, 1 to 4 blocks per SM,
+    ragged grids) gives the bits of the simulation run alone."""
     probs = [problems.blast_wave(12, seed=3), problems.blast_wave(10, seed=5)]
     ref = [alone(p, 4, precision)[0] for p in probs]
-    for v in range(8):
+    for v in range(10):
         b = Batch(3, precision=precision, arena_bytes=256 << 20, max_sims=4)
         slots = [b.add(p, 4) for p in probs]
         b.set_variant(v)
