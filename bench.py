@@ -157,7 +157,7 @@ def cpu_throughput(procs: int | None = None, budget_s: float = 4.0):
 
 
 def cpu_c1(nsteps: int = 2):
-    """configs[0] on the host: Orszag-Tang 256^2 through the reference's CPU
+    """The Orszag-Tang 256^2 workload on the host, through the reference's CPU
     build, `nsteps` RK4-equivalent steps, on 1 process and on nproc processes
     (one independent copy of the simulation per core: the reference's host
     build is single-threaded)."""
@@ -545,7 +545,7 @@ def accuracy_study(prob, steps: int, device: int, modes=("dt_rule", "fixed_dt"),
 
 
 def run_c1(a, ctx):
-    """the Orszag-Tang vortex 256^2, periodic, hyperdiffusion on,
+    """The Orszag-Tang vortex 256^2, periodic, hyperdiffusion on,
     Courant 0.3, 1000 RK4 steps under the reference's dt rule, on the GPU
     through the single-simulation context (FP64 and mixed, CUDA events around
     the 1000 steps); the reference's CPU build on the same problem (a bounded
@@ -628,7 +628,7 @@ def run_blast(a, ctx):
     out["mixed_vs_fp64"] = out["mixed"]["value"] / out["fp64"]["value"]
     if a.accuracy_steps > 0 and ctx.rank == 0:
         out["accuracy"] = accuracy_study(prob, a.accuracy_steps, ctx.local)
-        if a.c2_accuracy_steps > 0:  # configs[1]: 500 steps at a fixed dt
+        if a.c2_accuracy_steps > 0:  # the 128^3 blast wave: 500 steps at a fixed dt
             out["accuracy_500_steps_fixed_dt"] = accuracy_study(prob, a.c2_accuracy_steps, ctx.local,
                                                                 modes=("fixed_dt",), dt_probe_steps=50)
     return out
