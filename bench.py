@@ -513,11 +513,13 @@ def field_errors(w, ref, nw):
     return [float(np.linalg.norm(x[f] - y[f]) / (norms[f] if norms[f] > 1e-9 * big else big)) for f in range(nw)]
 
 
-def accuracy_study(prob, steps: int, device: int, modes=("dt_rule", "fixed_dt"), dt_probe_steps: int | None = None):
+def accuracy_study(prob, steps: int, device: int, modes=("dt_rule", "fixed_dt"), dt_probe_steps: int | None = None,
+                   checkpoints=()):
     """Per-field errors (field_errors) of the mixed and the FP64-FMA states
     against the FMA-free FP64 build (bit-identical to the oracle) after
     `steps` RK4 steps, under the reference's dt rule and at a fixed dt (half
-    the dt the rule reaches after min(steps, dt_probe_steps) steps)."""
+    the dt the rule reaches after min(steps, dt_probe_steps) steps); the
+    largest field error of both at each of `checkpoints` (steps) as well."""
     from smaug_b200 import PREC_MIXED, Engine
 
     nw = 2 + 2 * prob.ndim
@@ -531,12 +533,22 @@ def accuracy_study(prob, steps: int, device: int, modes=("dt_rule", "fixed_dt"),
         ex = Engine(prob, rk4=True, exact=True, device=device, **kw)
         fa = Engine(prob, rk4=True, device=device, **kw)
         mi = Engine(prob, rk4=True, device=device, precision=PREC_MIXED, **kw)
+        done, by_step = 0, []
+        for n in [c for c in sorted(checkpoints) if 0 < c < steps]:
+            for e in (ex, fa, mi):
+                e.step(n - done)
+            done = n
+            w_n = ex.state()
+            by_step.append({"step": n, "mixed_max_rel_l2": max(field_errors(mi.state(), w_n, nw)),
+                            "fp64_fma_max_rel_l2": max(field_errors(fa.state(), w_n, nw))})
         for e in (ex, fa, mi):
-            e.step(steps)
+            e.step(steps - done)
         we = ex.state()
         rm, rf = field_errors(mi.state(), we, nw), field_errors(fa.state(), we, nw)
         out[mode] = {"mixed_max_rel_l2": max(rm), "mixed_rel_l2_per_field": rm, "fp64_fma_max_rel_l2": max(rf),
                      "meets_1e-5": max(rm) <= 1e-5}
+        if by_step:
+            out[mode]["by_step"] = by_step
         if mode == "fixed_dt":
             out[mode]["dt"] = dt_fixed
         for e in (ex, fa, mi):
@@ -575,7 +587,8 @@ def run_c1(a, ctx):
         except Exception as ex:  # the GPU numbers stand on their own
             out["cpu_reference"] = {"failed": str(ex)}
     if a.accuracy_steps > 0 and ctx.rank == 0:
-        out["accuracy_1000_steps"] = accuracy_study(prob, a.c1_steps, ctx.local, dt_probe_steps=50)
+        out["accuracy_1000_steps"] = accuracy_study(prob, a.c1_steps, ctx.local, dt_probe_steps=50,
+                                                    checkpoints=(10, 30, 100, 300))
     return out
 
 
@@ -630,7 +643,8 @@ def run_blast(a, ctx):
         out["accuracy"] = accuracy_study(prob, a.accuracy_steps, ctx.local)
         if a.c2_accuracy_steps > 0:  # the 128^3 blast wave: 500 steps at a fixed dt
             out["accuracy_500_steps_fixed_dt"] = accuracy_study(prob, a.c2_accuracy_steps, ctx.local,
-                                                                modes=("fixed_dt",), dt_probe_steps=50)
+                                                                modes=("fixed_dt",), dt_probe_steps=50,
+                                                                checkpoints=(10, 50, 100, 250))
     return out
 
 
