@@ -422,7 +422,7 @@ def run_plain(probs, prec, ctx, steps, warmup):
     return {"value": ctx.world * cells * steps / (ms_max / 1e3), "ms_per_step": ms_max / steps}
 
 
-E2E_STEP_EVERY = 8  # admissions between the steps queued while the ensemble uploads
+E2E_STEP_EVERY = 4  # admissions between the steps queued while the ensemble uploads (swept: 2, 4, 8, 16, 96)
 
 
 def e2e_pipeline(b, probs, ws, mets, outs, steps: int):
