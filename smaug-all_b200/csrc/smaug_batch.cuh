@@ -64,12 +64,13 @@ __host__ __device__ inline BatchVariant batch_variant(int D, int v) {
   }
 }
 
-// Default variant of a single simulation and of an untuned batch, per ndim
-// and precision (the fastest of the variants in a B200 sweep of RK stage 1:
-// 96 Orszag-Tang simulations 128^2..768^2, one 128^3 blast wave).  A batch
+// Default variant of a single simulation and of an untuned batch (the
+// serving loop's), per ndim and precision: the fastest of the variants in
+// B200 sweeps of RK stage 1 on 96 Orszag-Tang simulations 128^2..768^2, on
+// 48 driven atmosphere slices (the served mix) and on one 128^3 blast wave.  A batch
 // and a single-simulation context on the same variant give the same bits.
 __host__ __device__ inline int batch_default_variant(int D, bool mixed) {
-  if (D == 2) return mixed ? 8 : 0;
+  if (D == 2) return mixed ? 6 : 0;
   return mixed ? 6 : 9;
 }
 
